@@ -1,0 +1,388 @@
+#!/usr/bin/env python
+"""Benchmark of the fused compression-aware select -> project -> sum path.
+
+Workload (one "step"): the select_sum_query pipeline over 2^28 rows --
+select(x < 512) on x (uniform over 10 bits), project the hits onto y
+(uniform over 20 bits), agg_sum -- with both columns stored as
+dynamic_vbp_f<512,64,8>, decompression fused into the operator.  Inputs are
+seeded synthetic columns generated and compressed on the device; they are
+larger than L2 (1.0 GB compressed), so no flush is needed between steps.
+
+value: algorithmic GB/s = (compressed bytes of x + y + 8-B result) / kernel
+time, inputs resident in HBM.  e2e: the same through the public C ABI with
+host buffers: each step copies both compressed columns (and their block
+indexes) from pinned host memory, runs the operator and reads the sum back.
+
+`--impl reference` times the reference's own CPU implementation (the
+MorphStore operators compiled from source under oracle/_ref, or the C
+restatement of them when that library is absent) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_ROWS = 1 << 28
+X_BITS, Y_BITS, PRED = 10, 20, 512
+SEED_X, SEED_Y = 0x5EED0001, 0x5EED0002
+METRIC = "fused decompress+select+project+sum GB/s (2^28-row dynamic_vbp columns)"
+WORKLOAD = "select(x<512)->project(y)->agg_sum, 2^28 rows, x uniform 10-bit, y uniform 20-bit, both dynamic_vbp<512,64,8>"
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def _traffic_per_launch():
+    """DRAM bytes per launch of the fused kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "k_sps_dvbp_2p28.md")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_launch:"):
+                    return int(line.split(":")[1].strip())
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=2)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _dist():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+# ---------------------------------------------------------------------------
+# reference / CPU baseline
+# ---------------------------------------------------------------------------
+def _cpu_sample_rows():
+    return 1 << 24
+
+
+def _cpu_worker(args):
+    """One process: generate its shard, compress with the reference (untimed),
+    time the reference operators.  Returns (seconds, compressed bytes, sum)."""
+    shard, rows, kind = args
+    import oracle
+    orc = oracle.Oracle()
+    x = orc.uniform_bits(SEED_X + shard, X_BITS, rows)
+    y = orc.uniform_bits(SEED_Y + shard, Y_BITS, rows)
+    if kind == "reference":
+        ref = oracle.Reference(oracle.reference_path())
+        s, cnt, secs, cb = ref.bench_select_project_sum(x, y, PRED)
+        return secs, cb, s
+    # port: the C restatement (decompress both columns, then select/project/sum)
+    bx, mx = orc.compress(oracle.DYNAMIC_VBP, 0, x)
+    by, my = orc.compress(oracle.DYNAMIC_VBP, 0, y)
+    t0 = time.perf_counter()
+    dx = orc.decompress(oracle.DYNAMIC_VBP, 0, bx, mx)
+    dy = orc.decompress(oracle.DYNAMIC_VBP, 0, by, my)
+    s, _ = orc.select_project_sum(oracle.CMP_LT, PRED, dx, dy)
+    secs = time.perf_counter() - t0
+    return secs, mx[1] + my[1], s
+
+
+def cpu_baseline(procs: int, reps: int = 1):
+    import multiprocessing as mp
+    import oracle
+    kind = "reference" if oracle.reference_path() else "port"
+    rows = _cpu_sample_rows()
+    best = None
+    ctx = mp.get_context("spawn")
+    for _ in range(reps):
+        with ctx.Pool(procs) as pool:
+            res = pool.map(_cpu_worker, [(i, rows, kind) for i in range(procs)])
+        secs = max(r[0] for r in res)
+        bytes_ = sum(r[1] for r in res)
+        gbs = bytes_ / secs / 1e9
+        best = gbs if best is None else max(best, gbs)
+    isa = ""
+    if kind == "reference":
+        isa = "avx512" if oracle.host_has_avx512() else "avx2"
+    sample = (f"{procs} process(es) x {rows} rows (2^24) each, same shapes and seeds scheme as the workload; "
+              f"operator time only (inputs compressed beforehand); {kind}{'/' + isa if isa else ''}")
+    return {"value": round(best, 3), "unit": "GB/s", "cores": procs, "kind": kind, "sample": sample}
+
+
+def run_reference(args):
+    rank, world, _ = _dist()
+    if rank != 0:
+        return 0
+    procs = max(1, os.cpu_count() or 1)
+    vals = []
+    for _ in range(args.warmup):
+        cpu_baseline(procs)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        vals.append(cpu_baseline(procs)["value"])
+    wall = time.perf_counter() - t0
+    cb = cpu_baseline(1)
+    cb_all = {"value": max(vals), "unit": "GB/s", "cores": procs, "kind": cb["kind"],
+              "sample": f"each step: {procs} processes x 2^24 rows, reference operators on the host cores"}
+    line = {"metric": METRIC, "value": max(vals), "unit": "GB/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(1000 * wall / max(1, args.steps), 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "impl": "reference", "config": {"workload": WORKLOAD + " (CPU sample: 2^24 rows per process)",
+                                            "parallelism": f"{procs} host processes"},
+            "cpu_baseline": cb_all, "single_thread_gbs": cb["value"],
+            "e2e": {"value": max(vals), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def run_gpu(args):
+    import torch
+    rank, world, local = _dist()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    import engine_b200 as ms
+    lib = ms.lib()
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+    arena = ms.Arena(16 << 30)
+
+    # --- data: generated and compressed on the device (outside timing) -------
+    n = N_ROWS
+    xu = arena.alloc(8 * n)
+    yu = arena.alloc(8 * n)
+    ms._check(lib.ms_gpu_gen_uniform_bits(SEED_X + rank, X_BITS, n, xu, sp), "gen x")
+    ms._check(lib.ms_gpu_gen_uniform_bits(SEED_Y + rank, Y_BITS, n, yu, sp), "gen y")
+    ux = ms.MsCol(format=ms.UNCOMPR, count_values=n, size_used_byte=8 * n, size_alloc_byte=8 * n, data=xu)
+    uy = ms.MsCol(format=ms.UNCOMPR, count_values=n, size_used_byte=8 * n, size_alloc_byte=8 * n, data=yu)
+    xc, yc = ms.MsCol(), ms.MsCol()
+    ms._check(lib.ms_gpu_morph(C.byref(ux), ms.DYNAMIC_VBP, 0, C.byref(xc), arena.h, sp), "morph x")
+    ms._check(lib.ms_gpu_morph(C.byref(uy), ms.DYNAMIC_VBP, 0, C.byref(yc), arena.h, sp), "morph y")
+    algo_bytes = int(xc.size_used_byte) + int(yc.size_used_byte) + 8
+
+    # expected result (device-side check with torch on the uncompressed inputs)
+    tx = ms._device_view(xu, 8 * n).view(torch.int64)
+    ty = ms._device_view(yu, 8 * n).view(torch.int64)
+    mask = tx < PRED
+    exp_sum = int(torch.where(mask, ty, torch.zeros_like(ty)).sum().item()) & ((1 << 64) - 1)
+    exp_cnt = int(mask.sum().item())
+    del tx, ty, mask
+
+    d_sum = arena.alloc(8)
+    d_cnt = arena.alloc(8)
+    d_err = arena.alloc(8)
+    torch.cuda.synchronize()
+
+    def step():
+        ms._check(lib.ms_gpu_select_project_sum_async(C.byref(xc), ms.less, PRED, C.byref(yc), d_sum, d_cnt, d_err,
+                                                      sp), "sps")
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    got_sum = int(ms._memcpy_d2h(d_sum, 8).view(np.uint64)[0])
+    got_cnt = int(ms._memcpy_d2h(d_cnt, 8).view(np.uint64)[0])
+    ok = (got_sum == exp_sum and got_cnt == exp_cnt)
+
+    # --- timed region: K steps, events around each launch ---------------------
+    if world > 1:
+        torch.distributed.barrier()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        t_all0 = torch.cuda.Event(enable_timing=True)
+        t_all1 = torch.cuda.Event(enable_timing=True)
+        t_all0.record(stream)
+        for i in range(args.steps):
+            ev[i][0].record(stream)
+            step()
+            ev[i][1].record(stream)
+        t_all1.record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    per = [a.elapsed_time(b) for a, b in ev]
+    total_ms = t_all0.elapsed_time(t_all1)
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    kern_ms = statistics.mean(per)
+    value = world * algo_bytes / (ms_per_step * 1e-3) / 1e9
+
+    # --- e2e: host buffers through the public API ----------------------------
+    e2e = e2e_run(ms, lib, arena, xc, yc, sp, args, exp_sum)
+
+    peak, peak_kind = _peaks()
+    achieved = algo_bytes / (kern_ms * 1e-3) / 1e9
+    line = {"metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "rows_per_gpu": n, "compressed_bytes_per_gpu": algo_bytes,
+                       "parallelism": f"replicas{world}" if world > 1 else "single",
+                       "l2": "inputs (1.0 GB) larger than L2; no flush"},
+            "parity": {"sum_ok": ok, "count": got_cnt},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                         "traffic": _traffic_per_launch(), "kernel": "k_sps<true,true> (ops.cu)",
+                         "algorithmic_bytes_per_launch": algo_bytes},
+            "clocks": clk.summary(), "e2e": e2e, "gpu_launches": args.steps}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            line["cpu_baseline"] = cpu_baseline(1)
+        except Exception as exc:  # baseline is reported, not required
+            line["cpu_baseline"] = {"error": str(exc)[:200]}
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    arena.close()
+    return 0 if ok else 1
+
+
+def e2e_run(ms, lib, arena, xc, yc, sp, args, exp_sum):
+    """Per step: H2D of both compressed columns + block indexes from pinned
+    host memory, the fused operator, D2H of the 8-byte sum."""
+    import torch
+    host = {}
+    for name, c in (("x", xc), ("y", yc)):
+        used = int(c.size_used_byte)
+        hb = torch.empty(used, dtype=torch.uint8, pin_memory=True)
+        hb.copy_(ms._device_view(c.data, used).cpu())
+        nb = int(c.n_index)
+        hi = torch.empty(8 * nb, dtype=torch.uint8, pin_memory=True)
+        idx = np.zeros(nb + 1, dtype=np.uint64)
+        hnp = hb.numpy()
+        ms._check(lib.ms_host_build_index(int(c.format), hnp.ctypes.data, int(c.size_compr_byte),
+                                          nb * 512, idx.ctypes.data, None), "host index")
+        hi.copy_(torch.from_numpy(idx[:nb].view(np.uint8)))
+        dbuf = arena.alloc(used + 64)
+        didx = arena.alloc(8 * nb + 8)
+        desc = ms.MsCol(format=c.format, bw=c.bw, count_values=c.count_values, size_used_byte=used,
+                        size_compr_byte=c.size_compr_byte, size_alloc_byte=used + 64, data=dbuf, index=didx,
+                        n_index=nb)
+        host[name] = (hb, hi, dbuf, didx, desc)
+    d_sum = arena.alloc(8)
+    d_err = arena.alloc(8)
+    h_sum = torch.empty(8, dtype=torch.uint8, pin_memory=True)
+    stream = torch.cuda.current_stream()
+    h2d = sum(h[0].numel() + h[1].numel() for h in host.values())
+    algo = int(xc.size_used_byte) + int(yc.size_used_byte) + 8
+
+    def step():
+        for hb, hi, dbuf, didx, desc in host.values():
+            ms._device_view(dbuf, hb.numel()).copy_(hb, non_blocking=True)
+            ms._device_view(didx, hi.numel()).copy_(hi, non_blocking=True)
+        ms._check(lib.ms_gpu_select_project_sum_async(C.byref(host["x"][4]), ms.less, PRED, C.byref(host["y"][4]),
+                                                      d_sum, None, d_err, sp), "sps e2e")
+        h_sum.copy_(ms._device_view(d_sum, 8), non_blocking=True)
+
+    for _ in range(2):
+        step()
+    torch.cuda.synchronize()
+    ok = int(h_sum.numpy().view(np.uint64)[0]) == exp_sum
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    k = max(1, min(args.steps, 20))
+    e0.record(stream)
+    for _ in range(k):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_step = e0.elapsed_time(e1) / k
+    return {"value": round(algo / (ms_step * 1e-3) / 1e9, 2), "unit": "GB/s", "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": 8, "ms_per_step": round(ms_step, 3), "sum_ok": ok,
+            "path": "ms_gpu_select_project_sum_async via ctypes, pinned host buffers"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_gpu(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

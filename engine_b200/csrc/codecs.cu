@@ -1,0 +1,555 @@
+// codecs.cu -- compression and decompression kernels for every format and
+// the column-level morph (morph.h:81-241).
+//
+// Encoding a dynamic_vbp-family column is size-then-scatter:
+//   1. k_analyze: one warp per 512-value block computes the block's bit width
+//      (OR-reduce, dynamic_vbp.h:124-158) after the cascade transform
+//      (delta: x[i]-x[i-8], delta.h:107-156; for: minus the block minimum,
+//      for.h:121-161);
+//   2. an exclusive scan of the bit widths gives every block's byte offset:
+//      64 * (headers before the block) + 64 * (sum of earlier widths);
+//   3. k_pack: one thread per lane stream (8 per block) packs the block at
+//      its offset and records the block index entry; k_headers writes the
+//      page headers (bit-width bytes / 0xFF, FOR reference words).
+// The same encoder writes operator outputs with the write iterator's
+// 2048-value chunking (write_iterator.h:67-306): only the number of blocks
+// per page changes (64 -> 4 for dynamic_vbp, 8 -> 2 for for_f).
+#include <string.h>
+
+#include "internal.h"
+#include "scan.cuh"
+
+namespace ms {
+namespace {
+
+struct Layout {
+    int fmt;
+    unsigned bw;           // static_vbp
+    unsigned dvbp_page;    // blocks per dynamic_vbp page (64 morph, 4 write iterator)
+    unsigned for_page;     // cascade blocks per for_f page (8 morph, 2 write iterator)
+};
+
+// 64-B headers preceding block b's packed data.
+__host__ __device__ inline uint64_t headers_before(const Layout &L, uint64_t b) {
+    switch (L.fmt) {
+    case MS_FMT_DYNAMIC_VBP: return b / L.dvbp_page + 1;
+    case MS_FMT_DELTA_DVBP: return b / 2 + 1;
+    case MS_FMT_FOR_DVBP: return b / (2 * L.for_page) + 1 + b / 2 + 1;
+    default: return 0;
+    }
+}
+
+__device__ __forceinline__ uint64_t warp_or(uint64_t x) {
+#pragma unroll
+    for (int s = 16; s > 0; s >>= 1) x |= __shfl_xor_sync(0xFFFFFFFFu, x, s);
+    return x;
+}
+
+// --- 1. analysis -----------------------------------------------------------
+// dynamic_vbp / delta: one warp per 512-block.
+template <int FMT>
+__global__ void __launch_bounds__(256) k_analyze_blocks(const uint64_t *__restrict__ in, uint64_t nb,
+                                                       uint32_t *__restrict__ bw_out) {
+    const unsigned lane = threadIdx.x & 31u;
+    for (uint64_t b = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) / 32; b < nb;
+         b += uint64_t(gridDim.x) * blockDim.x / 32) {
+        const uint64_t *blk = in + b * kBlock;
+        uint64_t acc = 1;
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+            const unsigned r = k * 32 + lane;  // coalesced rows
+            uint64_t x = __ldg(blk + r);
+            if (FMT == MS_FMT_DELTA_DVBP) {
+                const uint64_t row = b * kBlock + r;
+                x -= row >= 8 ? __ldg(in + row - 8) : 0;
+            }
+            acc |= x;
+        }
+        acc = warp_or(acc);
+        if (lane == 0) bw_out[b] = effective_bitwidth(acc);
+    }
+}
+
+// for_f: one warp per 1024-block; reference = AVX-512 TVL minimum (signed
+// per lane, _mm512_min_epi64, then unsigned across lanes; for.h:121-161).
+__global__ void __launch_bounds__(256) k_analyze_for(const uint64_t *__restrict__ in, uint64_t ncb,
+                                                    uint32_t *__restrict__ bw_out, uint64_t *__restrict__ refs) {
+    const unsigned lane = threadIdx.x & 31u;
+    for (uint64_t c = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) / 32; c < ncb;
+         c += uint64_t(gridDim.x) * blockDim.x / 32) {
+        const uint64_t *blk = in + c * kCascBlock;
+        // lane & 7 is the TVL lane of every row this thread reads
+        int64_t mn = INT64_MAX;
+        uint64_t x[32];
+#pragma unroll
+        for (int k = 0; k < 32; k++) {
+            x[k] = __ldg(blk + k * 32 + lane);
+            mn = min(mn, (int64_t)x[k]);
+        }
+        mn = min(mn, (int64_t)__shfl_xor_sync(0xFFFFFFFFu, (uint64_t)mn, 8));
+        mn = min(mn, (int64_t)__shfl_xor_sync(0xFFFFFFFFu, (uint64_t)mn, 16));
+        uint64_t um = (uint64_t)mn;
+        um = min(um, __shfl_xor_sync(0xFFFFFFFFu, um, 1));
+        um = min(um, __shfl_xor_sync(0xFFFFFFFFu, um, 2));
+        um = min(um, __shfl_xor_sync(0xFFFFFFFFu, um, 4));
+        if (um == ~uint64_t(0)) um--;
+        uint64_t o0 = 1, o1 = 1;
+#pragma unroll
+        for (int k = 0; k < 16; k++) o0 |= x[k] - um;
+#pragma unroll
+        for (int k = 16; k < 32; k++) o1 |= x[k] - um;
+        o0 = warp_or(o0);
+        o1 = warp_or(o1);
+        if (lane == 0) {
+            refs[c] = um;
+            bw_out[2 * c] = effective_bitwidth(o0);
+            bw_out[2 * c + 1] = effective_bitwidth(o1);
+        }
+    }
+}
+
+// --- 3. packing -------------------------------------------------------------
+// Eight threads per block, one per lane stream; a warp packs four blocks.
+template <int FMT>
+__global__ void __launch_bounds__(256) k_pack(const uint64_t *__restrict__ in, uint64_t nb, Layout L,
+                                             const uint32_t *__restrict__ bws, const uint64_t *__restrict__ prefix,
+                                             const uint64_t *__restrict__ refs, uint8_t *__restrict__ out,
+                                             uint64_t *__restrict__ index, unsigned *err) {
+    const unsigned l = threadIdx.x & 7u;
+    for (uint64_t b = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) / 8; b < nb;
+         b += uint64_t(gridDim.x) * blockDim.x / 8) {
+        unsigned bw;
+        uint64_t off;
+        if (FMT == MS_FMT_STATIC_VBP) {
+            bw = L.bw;
+            off = b * 64ull * bw;
+        } else {
+            bw = bws[b];
+            off = 64ull * headers_before(L, b) + 64ull * prefix[b];
+            if (l == 0 && index) index[b] = idx_pack(off, bw);
+        }
+        const uint64_t *blk = in + b * kBlock;
+        const uint64_t ref = FMT == MS_FMT_FOR_DVBP ? refs[b >> 1] : 0;
+        auto get = [&](unsigned v) -> uint64_t {
+            const unsigned r = v * 8 + l;
+            uint64_t x = __ldg(blk + r);
+            if (FMT == MS_FMT_DELTA_DVBP) {
+                const uint64_t row = b * kBlock + r;
+                x -= row >= 8 ? __ldg(in + row - 8) : 0;
+            } else if (FMT == MS_FMT_FOR_DVBP) {
+                x -= ref;
+            }
+            return x;
+        };
+        if (!vbp_pack_lane_rt(bw, get, reinterpret_cast<uint64_t *>(out + off), l)) atomicOr(err, kErrCorrupt);
+    }
+}
+
+// Page headers.  dynamic_vbp: one thread per header byte.
+__global__ void k_headers_dvbp(uint64_t nb, Layout L, const uint32_t *__restrict__ bws,
+                               const uint64_t *__restrict__ prefix, uint8_t *__restrict__ out) {
+    const uint64_t pages = (nb + L.dvbp_page - 1) / L.dvbp_page;
+    for (uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < pages * kPageBlocks;
+         t += uint64_t(gridDim.x) * blockDim.x) {
+        const uint64_t p = t / kPageBlocks, j = t % kPageBlocks, b0 = p * L.dvbp_page;
+        const uint64_t start = 64ull * headers_before(L, b0) + 64ull * prefix[b0] - 64;
+        const uint64_t b = b0 + j;
+        out[start + j] = (j < L.dvbp_page && b < nb) ? uint8_t(bws[b]) : uint8_t(kNoBlock);
+    }
+}
+
+// delta / for: inner dynamic_vbp header of each 1024-block (2 widths + 62 x
+// 0xFF) and, for for_f, the page header of reference words.
+template <int FMT>
+__global__ void k_headers_casc(uint64_t nb, Layout L, const uint32_t *__restrict__ bws,
+                               const uint64_t *__restrict__ prefix, const uint64_t *__restrict__ refs,
+                               uint8_t *__restrict__ out) {
+    const uint64_t ncb = nb / 2;
+    for (uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < ncb * 8;
+         t += uint64_t(gridDim.x) * blockDim.x) {
+        const uint64_t c = t / 8, w = t % 8;
+        const uint64_t start = 64ull * headers_before(L, 2 * c) + 64ull * prefix[2 * c] - 64;
+        uint64_t word = ~uint64_t(0);
+        if (w == 0) word = (~uint64_t(0) << 16) | uint64_t(bws[2 * c] & 0xFF) | (uint64_t(bws[2 * c + 1] & 0xFF) << 8);
+        reinterpret_cast<uint64_t *>(out + start)[w] = word;
+        if (FMT == MS_FMT_FOR_DVBP && c % L.for_page == 0) {
+            const uint64_t fstart = start - 64;
+            const uint64_t nbp = minu(L.for_page, ncb - c);
+            uint64_t fw;
+            if (w < nbp) fw = refs[c + w];
+            else if (w == nbp) fw = ~uint64_t(0);
+            else fw = 0;
+            reinterpret_cast<uint64_t *>(out + fstart)[w] = fw;
+        }
+    }
+}
+
+// Uncompressed rest: copied behind the gap (morph.h:186-189,
+// write_iterator.h:157-170).  The compressed size is read on the device.
+__global__ void k_copy_rest(const uint64_t *__restrict__ in, uint64_t nrest, int fmt, unsigned bw,
+                            const uint64_t *__restrict__ d_compr, uint8_t *__restrict__ out) {
+    const uint64_t ro = rest_offset(fmt, bw, *d_compr);
+    uint64_t *dst = reinterpret_cast<uint64_t *>(out + ro);
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nrest; i += uint64_t(gridDim.x) * blockDim.x)
+        dst[i] = in[i];
+}
+
+__global__ void k_finish_sizes(uint64_t nb, Layout L, const uint32_t *__restrict__ bws,
+                               const uint64_t *__restrict__ prefix, uint64_t *__restrict__ d_compr) {
+    if (threadIdx.x || blockIdx.x) return;
+    if (nb == 0) {
+        *d_compr = 0;
+        return;
+    }
+    if (L.fmt == MS_FMT_STATIC_VBP) {
+        *d_compr = nb * 64ull * L.bw;
+        return;
+    }
+    *d_compr = 64ull * headers_before(L, nb - 1) + 64ull * prefix[nb - 1] + 64ull * bws[nb - 1];
+}
+
+// --- decompression ------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_decode_all(ColView c, uint64_t *__restrict__ out, unsigned *err) {
+    const unsigned lane = threadIdx.x & 31u, l = lane & 7u, q = lane >> 3;
+    const uint64_t nbt = c.nblocks_total();
+    for (uint64_t b = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) / 32; b < nbt;
+         b += uint64_t(gridDim.x) * blockDim.x / 32) {
+        uint64_t v[16];
+        unsigned valid;
+        if (!decode_block(c, b, l, q, v, valid) && lane == 0) atomicOr(err, kErrCorrupt);
+        const uint64_t row0 = b * kBlock;
+#pragma unroll
+        for (int k = 0; k < 16; k++)
+            if ((valid >> k) & 1u) out[row0 + (16u * q + k) * 8u + l] = v[k];
+    }
+}
+
+// --- rle ----------------------------------------------------------------------
+constexpr unsigned kRleTile = 4096;
+
+__device__ __forceinline__ bool rle_head(const uint64_t *in, uint64_t i) { return i == 0 || in[i] != in[i - 1]; }
+
+__global__ void __launch_bounds__(256) k_rle_count(const uint64_t *__restrict__ in, uint64_t n,
+                                                  uint32_t *__restrict__ tile_counts) {
+    __shared__ unsigned cnt;
+    if (threadIdx.x == 0) cnt = 0;
+    __syncthreads();
+    const uint64_t base = uint64_t(blockIdx.x) * kRleTile;
+    unsigned c = 0;
+    for (unsigned i = threadIdx.x; i < kRleTile; i += blockDim.x) {
+        const uint64_t r = base + i;
+        if (r < n && rle_head(in, r)) c++;
+    }
+    c = __reduce_add_sync(0xFFFFFFFFu, c);
+    if ((threadIdx.x & 31u) == 0) atomicAdd(&cnt, c);
+    __syncthreads();
+    if (threadIdx.x == 0) tile_counts[blockIdx.x] = cnt;
+}
+
+// Writes run starts in order: thread i of the tile handles rows base + 16*i..+15.
+__global__ void __launch_bounds__(256) k_rle_starts(const uint64_t *__restrict__ in, uint64_t n,
+                                                   const uint64_t *__restrict__ tile_off,
+                                                   uint64_t *__restrict__ starts) {
+    __shared__ unsigned warp_tot[8];
+    const uint64_t base = uint64_t(blockIdx.x) * kRleTile + threadIdx.x * 16u;
+    unsigned m = 0;
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+        const uint64_t r = base + k;
+        if (r < n && rle_head(in, r)) m |= 1u << k;
+    }
+    unsigned c = __popc(m), incl = c;
+    const unsigned lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int s = 1; s < 32; s <<= 1) {
+        unsigned t = __shfl_up_sync(0xFFFFFFFFu, incl, s);
+        if (lane >= unsigned(s)) incl += t;
+    }
+    if (lane == 31) warp_tot[wid] = incl;
+    __syncthreads();
+    unsigned wpre = 0;
+    for (unsigned w = 0; w < wid; w++) wpre += warp_tot[w];
+    uint64_t pos = tile_off[blockIdx.x] + wpre + incl - c;
+    while (m) {
+        const int k = __ffs(m) - 1;
+        starts[pos++] = base + k;
+        m &= m - 1;
+    }
+}
+
+__global__ void k_rle_pairs(const uint64_t *__restrict__ in, uint64_t n, const uint64_t *__restrict__ starts,
+                            const uint64_t *__restrict__ d_runs, uint64_t *__restrict__ out) {
+    const uint64_t runs = *d_runs;
+    for (uint64_t k = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < runs; k += uint64_t(gridDim.x) * blockDim.x) {
+        const uint64_t s = starts[k], e = k + 1 < runs ? starts[k + 1] : n;
+        out[2 * k] = in[s];
+        out[2 * k + 1] = e - s;
+    }
+}
+
+__global__ void k_rle_lengths(const uint64_t *__restrict__ pairs, uint64_t runs, uint64_t *__restrict__ lens) {
+    for (uint64_t k = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < runs; k += uint64_t(gridDim.x) * blockDim.x)
+        lens[k] = pairs[2 * k + 1];
+}
+
+// Expand runs: each CTA writes one tile of output rows; the tile's first
+// run is found by binary search over the run starts.
+__global__ void __launch_bounds__(256) k_rle_expand(const uint64_t *__restrict__ pairs,
+                                                   const uint64_t *__restrict__ rstart, uint64_t runs, uint64_t n,
+                                                   uint64_t *__restrict__ out) {
+    __shared__ uint64_t s_lo, s_hi;
+    const uint64_t t0 = uint64_t(blockIdx.x) * kRleTile;
+    if (t0 >= n) return;
+    const uint64_t t1 = minu(n, t0 + kRleTile);
+    if (threadIdx.x == 0) {
+        // last run with start <= t0
+        uint64_t lo = 0, hi = runs;
+        while (hi - lo > 1) {
+            uint64_t mid = (lo + hi) / 2;
+            if (rstart[mid] <= t0) lo = mid;
+            else hi = mid;
+        }
+        s_lo = lo;
+        lo = s_lo;
+        hi = runs;
+        while (hi - lo > 1) {
+            uint64_t mid = (lo + hi) / 2;
+            if (rstart[mid] <= t1 - 1) lo = mid;
+            else hi = mid;
+        }
+        s_hi = lo;
+    }
+    __syncthreads();
+    const uint64_t lo0 = s_lo, hi0 = s_hi;
+    for (uint64_t r = t0 + threadIdx.x; r < t1; r += blockDim.x) {
+        uint64_t lo = lo0, hi = hi0 + 1;
+        while (hi - lo > 1) {
+            uint64_t mid = (lo + hi) / 2;
+            if (rstart[mid] <= r) lo = mid;
+            else hi = mid;
+        }
+        out[r] = pairs[2 * lo];
+    }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// host drivers
+// ---------------------------------------------------------------------------
+static int encode_rle(const uint64_t *d_in, uint64_t n, ms_col *out, ms_arena *a, cudaStream_t st) {
+    const uint64_t tiles = (n + kRleTile - 1) / kRleTile;
+    uint8_t *data = arena_take_t<uint8_t>(a, 16 * n + 64);
+    uint32_t *tc = arena_take_t<uint32_t>(a, tiles + 1);
+    uint64_t *toff = arena_take_t<uint64_t>(a, tiles + 1);
+    uint64_t *d_runs = arena_take_t<uint64_t>(a, 1);
+    uint64_t *scr = arena_take_t<uint64_t>(a, scan_scratch_words(tiles, 1));
+    uint64_t *starts = arena_take_t<uint64_t>(a, n + 1);
+    if (!data || !tc || !toff || !d_runs || !scr || !starts) return ms_fail(MS_ERR_NOMEM, "arena exhausted (rle)");
+    uint64_t runs = 0;
+    if (n) {
+        k_rle_count<<<unsigned(tiles), 256, 0, st>>>(d_in, n, tc);
+        MS_CUDA_TRY(cudaGetLastError());
+        MS_CUDA_TRY((scan_exclusive<uint32_t, 1>(tc, tiles, toff, d_runs, scr, st)));
+        k_rle_starts<<<unsigned(tiles), 256, 0, st>>>(d_in, n, toff, starts);
+        MS_CUDA_TRY(cudaGetLastError());
+        k_rle_pairs<<<persistent_grid(256, 4), 256, 0, st>>>(d_in, n, starts, d_runs, (uint64_t *)data);
+        MS_CUDA_TRY(cudaGetLastError());
+        MS_CUDA_TRY(cudaMemcpyAsync(&runs, d_runs, 8, cudaMemcpyDeviceToHost, st));
+        MS_CUDA_TRY(cudaStreamSynchronize(st));
+    }
+    *out = ms_col{};
+    out->format = MS_FMT_RLE;
+    out->count_values = n;
+    out->size_used_byte = 16 * runs;
+    out->size_compr_byte = 16 * runs;
+    out->size_alloc_byte = 16 * n + 64;
+    out->data = data;
+    return MS_OK;
+}
+
+static int decode_rle(const ms_col *in, uint64_t *d_out, ms_arena *a, cudaStream_t st) {
+    const uint64_t runs = in->size_used_byte / 16, n = in->count_values;
+    if (!n) return MS_OK;
+    if (!runs) return ms_fail(MS_ERR_CORRUPT, "rle column with values but no runs");
+    uint64_t *lens = arena_take_t<uint64_t>(a, runs + 1);
+    uint64_t *rstart = arena_take_t<uint64_t>(a, runs + 1);
+    uint64_t *tot = arena_take_t<uint64_t>(a, 1);
+    uint64_t *scr = arena_take_t<uint64_t>(a, scan_scratch_words(runs, 1));
+    if (!lens || !rstart || !tot || !scr) return ms_fail(MS_ERR_NOMEM, "arena exhausted (rle decode)");
+    k_rle_lengths<<<persistent_grid(256, 4), 256, 0, st>>>((const uint64_t *)in->data, runs, lens);
+    MS_CUDA_TRY(cudaGetLastError());
+    MS_CUDA_TRY((scan_exclusive<uint64_t, 1>(lens, runs, rstart, tot, scr, st)));
+    const uint64_t tiles = (n + kRleTile - 1) / kRleTile;
+    k_rle_expand<<<unsigned(tiles), 256, 0, st>>>((const uint64_t *)in->data, rstart, runs, n, d_out);
+    MS_CUDA_TRY(cudaGetLastError());
+    return MS_OK;
+}
+
+// Shared encoder: `ncompr` rows (a block multiple) go to the compressed part
+// with page layout L, rows [ncompr, n) to the uncompressed rest.
+static int encode(const uint64_t *d_in, uint64_t n, uint64_t ncompr, Layout L, ms_col *out, ms_arena *a,
+                  cudaStream_t st) {
+    const int fmt = L.fmt;
+    const uint64_t nb = ncompr / kBlock;
+    const uint64_t cap = ms_size_max_byte_any_len(fmt, L.bw, n);
+    uint8_t *data = arena_take_t<uint8_t>(a, cap);
+    uint64_t *d_compr = arena_take_t<uint64_t>(a, 1);
+    uint64_t *index = nullptr, *aux = nullptr;
+    uint32_t *bws = nullptr;
+    uint64_t *prefix = nullptr, *tot = nullptr, *scr = nullptr, *refs = nullptr;
+    if (!data || !d_compr) return ms_fail(MS_ERR_NOMEM, "arena exhausted (encode)");
+    const unsigned grid = persistent_grid(256, 8);
+    if (fmt != MS_FMT_STATIC_VBP && nb) {
+        index = arena_take_t<uint64_t>(a, nb + 1);
+        bws = arena_take_t<uint32_t>(a, nb + 1);
+        prefix = arena_take_t<uint64_t>(a, nb + 1);
+        tot = arena_take_t<uint64_t>(a, 1);
+        scr = arena_take_t<uint64_t>(a, scan_scratch_words(nb, 1));
+        if (fmt == MS_FMT_FOR_DVBP) aux = refs = arena_take_t<uint64_t>(a, nb / 2 + 1);
+        if (!index || !bws || !prefix || !tot || !scr || (fmt == MS_FMT_FOR_DVBP && !refs))
+            return ms_fail(MS_ERR_NOMEM, "arena exhausted (encode scratch)");
+        if (fmt == MS_FMT_DYNAMIC_VBP) k_analyze_blocks<MS_FMT_DYNAMIC_VBP><<<grid, 256, 0, st>>>(d_in, nb, bws);
+        else if (fmt == MS_FMT_DELTA_DVBP) k_analyze_blocks<MS_FMT_DELTA_DVBP><<<grid, 256, 0, st>>>(d_in, nb, bws);
+        else k_analyze_for<<<grid, 256, 0, st>>>(d_in, nb / 2, bws, refs);
+        MS_CUDA_TRY(cudaGetLastError());
+        MS_CUDA_TRY((scan_exclusive<uint32_t, 1>(bws, nb, prefix, tot, scr, st)));
+    }
+    if (nb) {
+        switch (fmt) {
+        case MS_FMT_STATIC_VBP:
+            k_pack<MS_FMT_STATIC_VBP><<<grid, 256, 0, st>>>(d_in, nb, L, bws, prefix, refs, data, index, a->d_err);
+            break;
+        case MS_FMT_DYNAMIC_VBP:
+            k_pack<MS_FMT_DYNAMIC_VBP><<<grid, 256, 0, st>>>(d_in, nb, L, bws, prefix, refs, data, index, a->d_err);
+            k_headers_dvbp<<<grid, 256, 0, st>>>(nb, L, bws, prefix, data);
+            break;
+        case MS_FMT_DELTA_DVBP:
+            k_pack<MS_FMT_DELTA_DVBP><<<grid, 256, 0, st>>>(d_in, nb, L, bws, prefix, refs, data, index, a->d_err);
+            k_headers_casc<MS_FMT_DELTA_DVBP><<<grid, 256, 0, st>>>(nb, L, bws, prefix, refs, data);
+            break;
+        case MS_FMT_FOR_DVBP:
+            k_pack<MS_FMT_FOR_DVBP><<<grid, 256, 0, st>>>(d_in, nb, L, bws, prefix, refs, data, index, a->d_err);
+            k_headers_casc<MS_FMT_FOR_DVBP><<<grid, 256, 0, st>>>(nb, L, bws, prefix, refs, data);
+            break;
+        }
+        MS_CUDA_TRY(cudaGetLastError());
+    }
+    k_finish_sizes<<<1, 32, 0, st>>>(nb, L, bws, prefix, d_compr);
+    MS_CUDA_TRY(cudaGetLastError());
+    const uint64_t nrest = n - ncompr;
+    if (nrest) {
+        k_copy_rest<<<(unsigned)minu((nrest + 255) / 256, 1024), 256, 0, st>>>(d_in + ncompr, nrest, fmt, L.bw,
+                                                                                     d_compr, data);
+        MS_CUDA_TRY(cudaGetLastError());
+    }
+    uint64_t compr = 0;
+    MS_CUDA_TRY(cudaMemcpyAsync(&compr, d_compr, 8, cudaMemcpyDeviceToHost, st));
+    int rc = read_err(a, st);  // synchronises
+    if (rc) return rc;
+    *out = ms_col{};
+    out->format = uint32_t(fmt);
+    out->bw = fmt == MS_FMT_STATIC_VBP ? L.bw : 0;
+    out->count_values = n;
+    out->size_compr_byte = compr;
+    out->size_used_byte = nrest ? rest_offset(fmt, L.bw, compr) + 8 * nrest : compr;
+    out->size_alloc_byte = cap;
+    out->data = data;
+    out->index = index;
+    out->index_aux = aux;
+    out->n_index = index ? nb : 0;
+    return MS_OK;
+}
+
+int compress_values(const uint64_t *d_in, uint64_t n, int fmt, unsigned bw, ms_col *out, ms_arena *a,
+                    cudaStream_t st) {
+    if (fmt == MS_FMT_RLE) return encode_rle(d_in, n, out, a, st);
+    if (fmt == MS_FMT_UNCOMPR) {
+        uint64_t *data = arena_take_t<uint64_t>(a, n + 1);
+        if (!data) return ms_fail(MS_ERR_NOMEM, "arena exhausted (copy)");
+        if (n) MS_CUDA_TRY(cudaMemcpyAsync(data, d_in, 8 * n, cudaMemcpyDeviceToDevice, st));
+        *out = ms_col{};
+        out->format = MS_FMT_UNCOMPR;
+        out->count_values = n;
+        out->size_used_byte = 8 * n;
+        out->size_alloc_byte = 8 * n;
+        out->data = data;
+        return MS_OK;
+    }
+    if (fmt == MS_FMT_STATIC_VBP && (bw < 1 || bw > 64)) return ms_fail(MS_ERR_INVALID, "static_vbp bw must be 1..64");
+    if (fmt < 0 || fmt > MS_FMT_RLE) return ms_fail(MS_ERR_INVALID, "unknown format");
+    const uint64_t b = block_size(fmt);
+    Layout L{fmt, bw, kPageBlocks, kForPageBlocks};
+    return encode(d_in, n, n / b * b, L, out, a, st);
+}
+
+int write_values(const uint64_t *d_vals, uint64_t n_vec, uint64_t n_scalar, int fmt, unsigned bw, ms_col *out,
+                 ms_arena *a, cudaStream_t st) {
+    const uint64_t n = n_vec + n_scalar;
+    if (fmt == MS_FMT_UNCOMPR) {
+        // uncompr write iterator: the values as they are (uncompr.h:126-237)
+        *out = ms_col{};
+        out->format = MS_FMT_UNCOMPR;
+        out->count_values = n;
+        out->size_used_byte = 8 * n;
+        out->size_alloc_byte = 8 * n;
+        out->data = const_cast<uint64_t *>(d_vals);
+        return MS_OK;
+    }
+    if (fmt == MS_FMT_RLE) return ms_fail(MS_ERR_UNSUPPORTED, "rle_f has no write iterator");
+    if (fmt == MS_FMT_STATIC_VBP && (bw < 1 || bw > 64)) return ms_fail(MS_ERR_INVALID, "static_vbp bw must be 1..64");
+    if (fmt < 0 || fmt > MS_FMT_RLE) return ms_fail(MS_ERR_INVALID, "unknown format");
+    const uint64_t b = block_size(fmt);
+    const uint64_t full = n_vec / kWiBuffer * kWiBuffer;
+    const uint64_t ncompr = full + (n_vec - full) / b * b;
+    Layout L{fmt, bw, kWiBuffer / kBlock, kWiBuffer / kCascBlock};
+    return encode(d_vals, n, ncompr, L, out, a, st);
+}
+
+int decompress_to(const ms_col *in, uint64_t *d_out, ms_arena *a, cudaStream_t st) {
+    if (in->format == MS_FMT_RLE) return decode_rle(in, d_out, a, st);
+    ColView v;
+    int rc = prepare_view(in, a, st, &v);
+    if (rc) return rc;
+    if (!v.n) return MS_OK;
+    const uint64_t nbt = v.nblocks_total();
+    const unsigned grid = (unsigned)minu((nbt + 7) / 8, persistent_grid(256, 8));
+    k_decode_all<<<grid, 256, 0, st>>>(v, d_out, a->d_err);
+    MS_CUDA_TRY(cudaGetLastError());
+    return MS_OK;
+}
+
+}  // namespace ms
+
+extern "C" int ms_gpu_morph(const ms_col *src, int dst_format, unsigned dst_bw, ms_col *out, ms_arena *a,
+                            void *stream) {
+    using namespace ms;
+    if (!src || !out || !a) return ms_fail(MS_ERR_INVALID, "morph: null argument");
+    int rc = check_col(src, false);
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    // morph from a format to itself returns the input (morph.h:133-160)
+    if (int(src->format) == dst_format && (dst_format != MS_FMT_STATIC_VBP || src->bw == dst_bw)) {
+        *out = *src;
+        return MS_OK;
+    }
+    if (src->format == MS_FMT_UNCOMPR)
+        return compress_values((const uint64_t *)src->data, src->count_values, dst_format, dst_bw, out, a, st);
+    // decompress (possibly followed by a compress into another format)
+    uint64_t *tmp = arena_take_t<uint64_t>(a, src->count_values + 1);
+    if (!tmp) return ms_fail(MS_ERR_NOMEM, "arena exhausted (morph)");
+    rc = decompress_to(src, tmp, a, st);
+    if (rc) return rc;
+    if (dst_format == MS_FMT_UNCOMPR) {
+        rc = read_err(a, st);
+        if (rc) return rc;
+        *out = ms_col{};
+        out->format = MS_FMT_UNCOMPR;
+        out->count_values = src->count_values;
+        out->size_used_byte = 8 * src->count_values;
+        out->size_alloc_byte = 8 * src->count_values;
+        out->data = tmp;
+        return MS_OK;
+    }
+    return compress_values(tmp, src->count_values, dst_format, dst_bw, out, a, st);
+}

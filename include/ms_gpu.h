@@ -1,0 +1,184 @@
+/*
+ * ms_gpu.h -- C ABI of the B200 compression-aware query path.
+ *
+ * Plain pointers and sizes only.  Every entry point is stream-ordered on the
+ * `stream` argument (a cudaStream_t passed as void*, NULL = legacy default
+ * stream) and returns an ms_status.  No exceptions cross this boundary; the
+ * C++ drop-in layer (engine_b200/include/morphstore_b200/) and the Python
+ * layer (engine_b200/__init__.py) turn a non-OK status into an exception, as
+ * the reference's host code signals errors with std::runtime_error.
+ *
+ * Columns live in device memory (HBM) and are described by ms_col, the
+ * device-resident counterpart of the reference's column<F>
+ * (include/core/storage/column.h:45-287).  Byte layouts are the reference's
+ * AVX-512 defaults (include/core/morphing/default_formats.h:35-82) and are
+ * bit-identical to what the reference writes:
+ *   MS_FMT_UNCOMPR      uncompr_f                                  (format.h:90-96)
+ *   MS_FMT_STATIC_VBP   static_vbp_f<vbp_l<bw,8>>, bw in 1..64     (static_vbp.h:61-68)
+ *   MS_FMT_DYNAMIC_VBP  dynamic_vbp_f<512,64,8>                    (dynamic_vbp.h:84-159)
+ *   MS_FMT_DELTA_DVBP   delta_f<1024,8,dynamic_vbp_f<512,64,8>>    (delta.h:79-157)
+ *   MS_FMT_FOR_DVBP     for_f<1024,8,dynamic_vbp_f<512,64,8>>      (for.h:85-164)
+ *   MS_FMT_RLE          rle_f                                      (rle.h:42-49)
+ * A compressed column is its compressed main part followed, at
+ * ms_rest_offset(), by an uncompressed rest (column.h:182-214).
+ */
+#ifndef MS_GPU_H
+#define MS_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MS_ABI_VERSION 1
+
+typedef enum ms_status {
+    MS_OK = 0,
+    MS_ERR_INVALID = 1,      /* bad argument (null pointer, unknown format, bw) */
+    MS_ERR_UNSUPPORTED = 2,  /* format combination the reference rejects too   */
+    MS_ERR_CUDA = 3,         /* a CUDA runtime call failed                      */
+    MS_ERR_NOMEM = 4,        /* arena or output capacity exhausted              */
+    MS_ERR_CORRUPT = 5,      /* a kernel found an invalid header / bit width    */
+    MS_ERR_TIMEOUT = 6       /* a bounded device-side wait gave up              */
+} ms_status;
+
+enum {
+    MS_FMT_UNCOMPR = 0,
+    MS_FMT_STATIC_VBP = 1,
+    MS_FMT_DYNAMIC_VBP = 2,
+    MS_FMT_DELTA_DVBP = 3,
+    MS_FMT_FOR_DVBP = 4,
+    MS_FMT_RLE = 5
+};
+
+/* Comparison of select (vectorlib::equal/less/lessequal/greater/greaterequal,
+ * include/vector/primitives/compare.h:22-76).  Values before the operator's
+ * scalar remainder compare as signed 64-bit integers and the remainder as
+ * unsigned, as in the reference's AVX-512 build (compare_avx512.h:35-111,
+ * compare_scalar.h:17-77); both agree for values below 2^63. */
+enum { MS_CMP_EQ = 0, MS_CMP_LT = 1, MS_CMP_LE = 2, MS_CMP_GT = 3, MS_CMP_GE = 4 };
+
+/* Device-resident column descriptor (column<F> metadata, column.h:133-144).
+ * `index` is an optional device array built by ms_gpu_build_index (or by the
+ * compressing morph): one uint64 per 512-value block of the compressed part,
+ * (byte offset of the packed block) | (bit width << 56); for MS_FMT_FOR_DVBP
+ * `index_aux` holds one reference value per 1024-value block. */
+typedef struct ms_col {
+    uint32_t format;
+    uint32_t bw;              /* static_vbp bit width, 0 otherwise */
+    uint64_t count_values;    /* m_CountLogicalValues */
+    uint64_t size_used_byte;  /* m_SizeUsedByte */
+    uint64_t size_compr_byte; /* m_SizeComprByte */
+    uint64_t size_alloc_byte; /* capacity of `data` */
+    void *data;               /* device pointer, 64-B aligned at least */
+    uint64_t *index;          /* optional, device; see above */
+    uint64_t *index_aux;      /* optional, device */
+    uint64_t n_index;         /* entries in `index` */
+} ms_col;
+
+/* Device memory arena: the device-resident replacement of the reference's
+ * query_memory_manager (include/core/memory/management/query_mm.h:83-238).
+ * One cudaMalloc at creation; ms_gpu_arena_alloc bumps; reset frees all. */
+typedef struct ms_arena ms_arena;
+
+/* ---- library / arena ------------------------------------------------------ */
+int ms_gpu_abi_version(void);
+const char *ms_gpu_status_string(int status);
+int ms_gpu_device_info(int *sm_count, int *cc_major, int *cc_minor);
+int ms_gpu_arena_create(uint64_t capacity_byte, ms_arena **out);
+int ms_gpu_arena_alloc(ms_arena *a, uint64_t size_byte, void **out);
+int ms_gpu_arena_reset(ms_arena *a);
+int ms_gpu_arena_used(const ms_arena *a, uint64_t *used_byte);
+int ms_gpu_arena_destroy(ms_arena *a);
+/* Synchronise `stream` and report (then clear) errors that asynchronous
+ * kernels recorded in the arena's device error word. */
+int ms_gpu_arena_check(ms_arena *a, void *stream);
+
+/* ---- layout arithmetic (host only) --------------------------------------- */
+/* get_size_max_byte_any_len<F>(n)  (include/core/morphing/format.h:114-153) */
+uint64_t ms_size_max_byte_any_len(int format, unsigned bw, uint64_t count_values);
+/* column<F>::create_data_uncompr_start as an offset (column.h:182-196) */
+uint64_t ms_rest_offset(int format, unsigned bw, uint64_t size_compr_byte);
+/* Host-side page walk that fills a host copy of ms_col.index from a host copy
+ * of the compressed bytes (no counterpart in the reference; it replaces the
+ * sequential header walk of dynamic_vbp.h:283-307 / for.h:297-360).
+ * `index` needs count_compr/512 entries, `aux` count_compr/1024 (FOR). */
+int ms_host_build_index(int format, const uint8_t *host_data, uint64_t size_compr_byte,
+                        uint64_t count_compr, uint64_t *index, uint64_t *aux);
+
+/* ---- morph (include/core/morphing/morph.h:81-241) -------------------------- */
+/* Compress an uncompressed device column into `dst_format`, or decompress a
+ * compressed one into uncompr_f.  `out` storage comes from the arena; on
+ * return *out is complete (the call synchronises `stream` to read back sizes).
+ * Compressing to a dynamic_vbp-family format also fills out->index. */
+int ms_gpu_morph(const ms_col *src, int dst_format, unsigned dst_bw, ms_col *out,
+                 ms_arena *arena, void *stream);
+/* Build ms_col.index for a device column (device-side page walk). */
+int ms_gpu_build_index(ms_col *col, ms_arena *arena, void *stream);
+
+/* ---- operators (include/core/operators/interfaces/*.h) ------------------- */
+/* agg_sum<ve,F>(col) (agg_sum.h:56-65; agg_sum_compr.h:78-153): the uint64
+ * wrapping sum written to device *d_sum (asynchronous; the arena supplies
+ * scratch such as delta carries; ms_gpu_arena_check reports kernel errors). */
+int ms_gpu_agg_sum(const ms_col *in, uint64_t *d_sum, ms_arena *arena, void *stream);
+
+/* my_select_wit_t<cmp,ve,out_f,in_f>::apply(in, val) (select_compr.h:100-260):
+ * ascending positions where cmp(value, val) holds, written in `out_format`
+ * with the reference write iterator's chunking (write_iterator.h:67-306). */
+int ms_gpu_select(int cmp, uint64_t val, const ms_col *in, int out_format, unsigned out_bw,
+                  ms_col *out, ms_arena *arena, void *stream);
+
+/* my_project_wit_t<ve,out_f,data_f,pos_f>::apply(data, pos)
+ * (project_compr.h:75-262).  Unlike the reference, data may also be a
+ * dynamic_vbp-family column (random access through ms_col.index). */
+int ms_gpu_project(const ms_col *data, const ms_col *pos, int out_format, unsigned out_bw,
+                   ms_col *out, ms_arena *arena, void *stream);
+
+/* The fused select -> project -> agg_sum pipeline of
+ * src/examples/select_sum_query.cpp:77-97: sum of y[i] over rows with
+ * cmp(x[i], c), without materialising positions.  x and y have the same
+ * count.  Optional outputs (NULL to skip): d_count, and uncompressed
+ * positions / projected values (device arrays of capacity >= count). */
+int ms_gpu_select_project_sum(const ms_col *x, int cmp, uint64_t c, const ms_col *y,
+                              uint64_t *d_sum, uint64_t *d_count, uint64_t *d_pos,
+                              uint64_t *d_vals, ms_arena *arena, void *stream);
+
+/* Launch-only form of the fused pipeline for graph capture and timing: no
+ * scratch, no synchronisation; x and y must be uncompr / static_vbp or carry
+ * a block index; kernel errors are OR-ed into device *d_err. */
+int ms_gpu_select_project_sum_async(const ms_col *x, int cmp, uint64_t c, const ms_col *y,
+                                    uint64_t *d_sum, uint64_t *d_count, unsigned *d_err, void *stream);
+
+/* semi_join<ve,out_f,L_f,R_f>(L, R) (join.h:193-218,
+ * join_semi_equi_compr.h:106-300): ascending positions of R whose value
+ * occurs in L. */
+int ms_gpu_semi_join(const ms_col *l, const ms_col *r, int out_format, unsigned out_bw,
+                     ms_col *out, ms_arena *arena, void *stream);
+
+/* intersect_sorted / my_intersect_wit_t (intersect.h:52-63,
+ * intersect_compr.h:190-347): sorted intersection of two position lists. */
+int ms_gpu_intersect_sorted(const ms_col *l, const ms_col *r, int out_format, unsigned out_bw,
+                            ms_col *out, ms_arena *arena, void *stream);
+
+/* group_vec<ve,gr_f,ext_f,in_f>(in) (group_compr.h:281-300) and the binary
+ * group (group.h:97-112, gr_in != NULL): group ids in order of first
+ * occurrence and the first position of every group. */
+int ms_gpu_group(const ms_col *gr_in, const ms_col *in, int gr_format, ms_col *out_gr,
+                 int ext_format, ms_col *out_ext, ms_arena *arena, void *stream);
+
+/* grouped agg_sum<ve>(gr, data, n_groups) (agg_sum.h:95-106,
+ * scalar/agg_sum_uncompr.h:64-95): uncompressed sums per group. */
+int ms_gpu_agg_sum_grouped(const ms_col *gr, const ms_col *data, uint64_t n_groups,
+                           ms_col *out, ms_arena *arena, void *stream);
+
+/* ---- synthetic data (device-side, counter-based splitmix64) -------------- */
+int ms_gpu_gen_uniform_bits(uint64_t seed, unsigned bits, uint64_t n, uint64_t *d_out, void *stream);
+int ms_gpu_gen_from_table(uint64_t seed, const uint64_t *d_table, uint64_t n_table, uint64_t n,
+                          uint64_t *d_out, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MS_GPU_H */

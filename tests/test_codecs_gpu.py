@@ -1,0 +1,103 @@
+"""GPU codec parity: bytes written by the CUDA encoders and values returned
+by the CUDA decoders, against the oracle on the same seeded inputs."""
+import numpy as np
+import pytest
+
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+LENGTHS = [0, 1, 17, 512, 1000, 1024, 2047, 4096 + 17, 33000, 70001]
+
+
+def _values(orc, fmt, bw, n, seed):
+    if fmt == O.STATIC_VBP:
+        return orc.uniform_bits(seed, bw, n)
+    if fmt == O.DELTA_DVBP:
+        return orc.sorted_gaps(seed, orc.geom_table(0.25), n)
+    if fmt == O.RLE:
+        return orc.runs(seed, 5, 20, n)
+    return orc.uniform_bits(seed, 20, n)
+
+
+def _masked(fmt, bw, data, meta, orc):
+    return O.mask_gap(fmt, bw, data, meta, orc)
+
+
+def _fmt(ms, fmt, bw):
+    return {O.UNCOMPR: ms.uncompr_f, O.STATIC_VBP: ms.static_vbp_f(bw) if bw else None,
+            O.DYNAMIC_VBP: ms.dynamic_vbp_f, O.DELTA_DVBP: ms.delta_f, O.FOR_DVBP: ms.for_f,
+            O.RLE: ms.rle_f}[fmt]
+
+
+@pytest.mark.parametrize("fmt", [O.DYNAMIC_VBP, O.DELTA_DVBP, O.FOR_DVBP, O.RLE])
+@pytest.mark.parametrize("n", LENGTHS)
+def test_compress_bytes_match_oracle(ms, arena, orc, fmt, n):
+    v = _values(orc, fmt, 0, n, seed=100 + n)
+    col = ms.Column.from_numpy(v, arena)
+    c = ms.morph(col, _fmt(ms, fmt, 0))
+    b, m = orc.compress(fmt, 0, v)
+    assert c.meta() == m
+    got = c.raw_bytes()
+    assert np.array_equal(_masked(fmt, 0, got, m, orc), _masked(fmt, 0, b, m, orc))
+    assert np.array_equal(c.to_numpy(), v)
+
+
+@pytest.mark.parametrize("bw", list(range(1, 65)))
+def test_static_vbp_every_bit_width(ms, arena, orc, bw):
+    n = 3 * 512 + 17
+    v = orc.uniform_bits(7 * bw, bw, n)
+    c = ms.morph(ms.Column.from_numpy(v, arena), ms.static_vbp_f(bw))
+    b, m = orc.compress(O.STATIC_VBP, bw, v)
+    assert c.meta() == m
+    assert np.array_equal(_masked(O.STATIC_VBP, bw, c.raw_bytes(), m, orc), _masked(O.STATIC_VBP, bw, b, m, orc))
+    assert np.array_equal(c.to_numpy(), v)
+
+
+@pytest.mark.parametrize("bits", [1, 8, 31, 32, 33, 63, 64])
+def test_dvbp_and_for_wide_values(ms, arena, orc, bits):
+    """Every block bit width, including 64-bit values (signed FOR minimum)."""
+    n = 8 * 1024 + 300
+    v = orc.uniform_bits(bits, bits, n)
+    for fmt in (O.DYNAMIC_VBP, O.FOR_DVBP, O.DELTA_DVBP):
+        c = ms.morph(ms.Column.from_numpy(v, arena), _fmt(ms, fmt, 0))
+        b, m = orc.compress(fmt, 0, v)
+        assert c.meta() == m, fmt
+        assert np.array_equal(_masked(fmt, 0, c.raw_bytes(), m, orc), _masked(fmt, 0, b, m, orc)), fmt
+        assert np.array_equal(c.to_numpy(), v), fmt
+
+
+@pytest.mark.parametrize("fmt", [O.DYNAMIC_VBP, O.DELTA_DVBP, O.FOR_DVBP])
+def test_decode_reference_bytes_with_host_index(ms, arena, orc, fmt):
+    """Columns uploaded in the reference layout decode through the host index."""
+    v = _values(orc, fmt, 0, 100_000 + 123, seed=5)
+    b, m = orc.compress(fmt, 0, v)
+    c = ms.Column.from_bytes(_fmt(ms, fmt, 0), b, m, arena)
+    assert np.array_equal(c.to_numpy(), v)
+    # and through the device-side page walk
+    c2 = ms.Column.from_bytes(_fmt(ms, fmt, 0), b, m, arena, build_index=False)
+    c2.build_index()
+    assert np.array_equal(c2.to_numpy(), v)
+
+
+def test_mixed_block_widths(ms, arena, orc):
+    """Blocks of different widths inside one dynamic_vbp page."""
+    n = 64 * 512 * 2 + 999
+    v = orc.uniform_bits(11, 64, n)
+    shifts = (np.arange(n) // 512) % 64
+    v = v >> shifts.astype(np.uint64)
+    for fmt in (O.DYNAMIC_VBP, O.FOR_DVBP):
+        c = ms.morph(ms.Column.from_numpy(v, arena), _fmt(ms, fmt, 0))
+        b, m = orc.compress(fmt, 0, v)
+        assert c.meta() == m
+        assert np.array_equal(_masked(fmt, 0, c.raw_bytes(), m, orc), _masked(fmt, 0, b, m, orc))
+        assert np.array_equal(c.to_numpy(), v)
+
+
+def test_compressed_to_compressed(ms, arena, orc):
+    v = _values(orc, O.DELTA_DVBP, 0, 50_000, seed=9)
+    a = ms.morph(ms.Column.from_numpy(v, arena), ms.delta_f)
+    bcol = ms.morph(a, ms.for_f)
+    b, m = orc.compress(O.FOR_DVBP, 0, v)
+    assert bcol.meta() == m
+    assert np.array_equal(bcol.to_numpy(), v)
