@@ -48,7 +48,26 @@ def build(verbose: bool = False) -> str:
     if not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
         cmd = [NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB, *objs]
         subprocess.run(cmd, check=True)
+    _build_examples()
     return LIB
+
+
+def _build_examples() -> None:
+    """The C++ drop-in examples, linked against libms_gpu.so."""
+    ex = os.path.join(HERE, "examples")
+    out = os.path.join(ex, "bin")
+    os.makedirs(out, exist_ok=True)
+    for src in sorted(f for f in os.listdir(ex) if f.endswith(".cpp")):
+        binp = os.path.join(out, src[:-4])
+        srcp = os.path.join(ex, src)
+        hdr = os.path.join(HERE, "include", "morphstore_b200", "morphstore.h")
+        if os.path.exists(binp) and os.path.getmtime(binp) > max(os.path.getmtime(srcp), os.path.getmtime(hdr),
+                                                                   os.path.getmtime(LIB)):
+            continue
+        cmd = ["g++", "-std=c++14", "-O2", "-Wall", "-I", os.path.join(HERE, "..", "include"),
+               "-I", os.path.join(HERE, "include"), srcp, "-o", binp, "-L", HERE, "-lms_gpu",
+               "-Wl,-rpath,$ORIGIN/../.."]
+        subprocess.run(cmd, check=True)
 
 
 if __name__ == "__main__":

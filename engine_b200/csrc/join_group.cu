@@ -303,7 +303,8 @@ __global__ void __launch_bounds__(256) k_group_insert(ColView gin, bool binary, 
 #pragma unroll
         for (int k = 0; k < 16; k++) {
             if (!((valid >> k) & 1u) || bad != kInsOk) continue;
-            bad = group_insert(t, binary ? g[k] : 0, v[k], row0 + (16u * q + k) * 8u + l);
+            // unary: the key lives in ka; binary: (group, value) in (ka, kb)
+            bad = group_insert(t, binary ? g[k] : v[k], binary ? v[k] : 0, row0 + (16u * q + k) * 8u + l);
         }
     }
     if (!ok) atomicOr(err, kErrCorrupt);
@@ -356,7 +357,7 @@ __global__ void __launch_bounds__(256) k_group_ids(ColView gin, bool binary, Col
         for (int k = 0; k < 16; k++) {
             if (!((valid >> k) & 1u)) continue;
             uint64_t slot = 0;
-            if (!group_find(t, binary ? g[k] : 0, v[k], slot)) {
+            if (!group_find(t, binary ? g[k] : v[k], binary ? v[k] : 0, slot)) {
                 ok = false;
                 continue;
             }

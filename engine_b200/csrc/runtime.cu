@@ -93,6 +93,22 @@ extern "C" int ms_gpu_arena_destroy(ms_arena *a) {
     return MS_OK;
 }
 
+extern "C" int ms_gpu_memcpy(void *dst, const void *src, uint64_t bytes, int kind, int sync, void *stream) {
+    if (!bytes) return MS_OK;
+    if (!dst || !src) return ms_fail(MS_ERR_INVALID, "memcpy: null pointer");
+    const cudaMemcpyKind k = kind == 0 ? cudaMemcpyHostToDevice : kind == 1 ? cudaMemcpyDeviceToHost
+                                                                            : cudaMemcpyDeviceToDevice;
+    if (kind < 0 || kind > 2) return ms_fail(MS_ERR_INVALID, "memcpy: unknown kind");
+    MS_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, k, (cudaStream_t)stream));
+    if (sync) MS_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+    return MS_OK;
+}
+
+extern "C" int ms_gpu_stream_sync(void *stream) {
+    MS_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+    return MS_OK;
+}
+
 int ms::read_err(ms_arena *a, cudaStream_t st) {
     unsigned h = 0;
     MS_CUDA_TRY(cudaMemcpyAsync(&h, a->d_err, sizeof h, cudaMemcpyDeviceToHost, st));

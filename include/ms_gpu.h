@@ -96,6 +96,12 @@ int ms_gpu_arena_destroy(ms_arena *a);
  * kernels recorded in the arena's device error word. */
 int ms_gpu_arena_check(ms_arena *a, void *stream);
 
+/* Copies between host and device memory for callers that do not include the
+ * CUDA headers (kind: 0 host->device, 1 device->host, 2 device->device);
+ * synchronous with respect to `stream` when `sync` is non-zero. */
+int ms_gpu_memcpy(void *dst, const void *src, uint64_t bytes, int kind, int sync, void *stream);
+int ms_gpu_stream_sync(void *stream);
+
 /* ---- layout arithmetic (host only) --------------------------------------- */
 /* get_size_max_byte_any_len<F>(n)  (include/core/morphing/format.h:114-153) */
 uint64_t ms_size_max_byte_any_len(int format, unsigned bw, uint64_t count_values);
@@ -118,7 +124,7 @@ int ms_gpu_morph(const ms_col *src, int dst_format, unsigned dst_bw, ms_col *out
 /* Build ms_col.index for a device column (device-side page walk). */
 int ms_gpu_build_index(ms_col *col, ms_arena *arena, void *stream);
 
-/* ---- operators (include/core/operators/interfaces/*.h) ------------------- */
+/* ---- operators (include/core/operators/interfaces/) ----------------------- */
 /* agg_sum<ve,F>(col) (agg_sum.h:56-65; agg_sum_compr.h:78-153): the uint64
  * wrapping sum written to device *d_sum (asynchronous; the arena supplies
  * scratch such as delta carries; ms_gpu_arena_check reports kernel errors). */

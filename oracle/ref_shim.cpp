@@ -146,6 +146,7 @@ extern "C" {
 // per range so the 64 instances compile in parallel).
 #define MS_CAT2(a, b) a##b
 #define MS_CAT(a, b) MS_CAT2(a, b)
+extern "C++" {
 template <class Fn, unsigned B> struct sv_part {
     static int go(unsigned bw, Fn &fn) {
         if (bw == B) return fn(tag<sv<B>>{});
@@ -155,6 +156,7 @@ template <class Fn, unsigned B> struct sv_part {
 template <class Fn> struct sv_part<Fn, PART_SV_HI + 1> {
     static int go(unsigned, Fn &) { return -10; }
 };
+}
 
 int MS_CAT(ref_sv_compress_, PART_SV_LO)(unsigned bw, const uint64_t *in, uint64_t n, uint8_t *out, uint64_t cap,
                                           ref_meta *m) {

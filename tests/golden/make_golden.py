@@ -1,0 +1,147 @@
+"""Generates the golden fixtures in this directory by running the MorphStore
+reference's own codecs and operators (AVX-512 build of oracle/ref_shim.cpp,
+compiled from the reference source tree by oracle/Makefile).
+
+    make -C oracle ref && python tests/golden/make_golden.py
+
+Inputs come from the oracle's seeded generators; outputs (compressed bytes,
+column metadata, positions, group ids, sums) come from the reference.  The
+fixtures pin the C oracle (tests/test_golden_cpu.py) and the CUDA path
+(tests/test_golden_gpu.py) without needing the reference at test time.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+import oracle as O  # noqa: E402
+
+OUT = os.path.join(HERE, "golden.npz")
+
+
+def inputs(orc):
+    """Named seeded input columns of the four distributions and odd lengths."""
+    geo4 = orc.geom_table(0.25)
+    zipf = orc.zipf_table(1.2, 1 << 20)
+    cols = {}
+    for n in (17, 1234, 4096 + 17, 33_000 + 9):
+        cols[f"uni20_{n}"] = orc.uniform_bits(n, 20, n)
+        cols[f"zipf_{n}"] = orc.from_table(n + 1, zipf, n)
+        cols[f"sorted_{n}"] = orc.sorted_gaps(n + 2, geo4, n)
+        cols[f"runs_{n}"] = orc.runs(n + 3, 5, 20, n)
+    cols["uni64_9000"] = orc.uniform_bits(64, 64, 9000)
+    cols["uni12_40077"] = orc.uniform_bits(12, 12, 40_077)
+    return cols
+
+
+def main():
+    path = O.reference_path("avx512")
+    if path is None:
+        raise SystemExit("build the reference first: make -C oracle ref")
+    ref = O.Reference(path)
+    orc = O.Oracle()
+    cols = inputs(orc)
+    fx = {}
+    for name, v in cols.items():
+        fx[f"in/{name}"] = v
+    # --- codecs ---------------------------------------------------------------
+    for name, v in cols.items():
+        fmts = [(O.DYNAMIC_VBP, 0), (O.DELTA_DVBP, 0), (O.FOR_DVBP, 0), (O.RLE, 0)]
+        if name.startswith("uni20"):
+            fmts += [(O.STATIC_VBP, 20), (O.STATIC_VBP, 33)]
+        if name == "uni64_9000":
+            fmts = [(O.STATIC_VBP, 64), (O.DYNAMIC_VBP, 0), (O.FOR_DVBP, 0), (O.DELTA_DVBP, 0)]
+        for fmt, bw in fmts:
+            b, m = ref.compress(fmt, bw, v)
+            key = f"codec/{name}/{fmt}/{bw}"
+            fx[key + "/bytes"] = O.mask_gap(fmt, bw, b, m, orc)
+            fx[key + "/meta"] = np.array(m, dtype=np.uint64)
+    for bw in range(1, 65):
+        v = orc.uniform_bits(1000 + bw, bw, 1024 + 37)
+        b, m = ref.compress(O.STATIC_VBP, bw, v)
+        fx[f"static/{bw}/in"] = v
+        fx[f"static/{bw}/bytes"] = O.mask_gap(O.STATIC_VBP, bw, b, m, orc)
+        fx[f"static/{bw}/meta"] = np.array(m, dtype=np.uint64)
+    # --- select with compressed inputs / outputs ----------------------------------
+    x = cols["uni12_40077"]
+    for in_fmt, in_bw in [(O.UNCOMPR, 0), (O.DYNAMIC_VBP, 0), (O.DELTA_DVBP, 0), (O.FOR_DVBP, 0)]:
+        if in_fmt == O.UNCOMPR:
+            xb, xm = x.view(np.uint8).copy(), (len(x), 8 * len(x), 0)
+        else:
+            xb, xm = ref.compress(in_fmt, in_bw, x)
+        for out_fmt in (O.UNCOMPR, O.DYNAMIC_VBP, O.DELTA_DVBP, O.FOR_DVBP):
+            ob, om = ref.select(O.CMP_LT, 1500, in_fmt, in_bw, xb, xm, out_fmt, 0)
+            key = f"select/{in_fmt}/{out_fmt}"
+            fx[key + "/bytes"] = O.mask_gap(out_fmt, 0, ob, om, orc)
+            fx[key + "/meta"] = np.array(om, dtype=np.uint64)
+    for cmp in range(5):
+        ob, om = ref.select(cmp, 2048, O.UNCOMPR, 0, x.view(np.uint8), (len(x), 8 * len(x), 0), O.UNCOMPR, 0)
+        fx[f"select_cmp/{cmp}"] = ob.view(np.uint64)
+    # --- select on values >= 2^63 (AVX-512 signed compare) -------------------------
+    w = cols["uni64_9000"]
+    ob, om = ref.select(O.CMP_LT, 1 << 62, O.UNCOMPR, 0, w.view(np.uint8), (len(w), 8 * len(w), 0), O.UNCOMPR, 0)
+    fx["select_signed"] = ob.view(np.uint64)
+    # --- project --------------------------------------------------------------------
+    y = cols["uni20_33009"]
+    yb, ym = ref.compress(O.STATIC_VBP, 20, y)
+    pos = np.arange(3, len(y), 7, dtype=np.uint64)
+    for out_fmt in (O.UNCOMPR, O.DYNAMIC_VBP):
+        ob, om = ref.project(O.STATIC_VBP, 20, yb, ym, O.UNCOMPR, 0, pos.view(np.uint8), (len(pos), 8 * len(pos), 0),
+                             out_fmt, 0)
+        fx[f"project/{out_fmt}/bytes"] = O.mask_gap(out_fmt, 0, ob, om, orc)
+        fx[f"project/{out_fmt}/meta"] = np.array(om, dtype=np.uint64)
+    # --- agg_sum ----------------------------------------------------------------------
+    for fmt in (O.UNCOMPR, O.DYNAMIC_VBP, O.DELTA_DVBP, O.FOR_DVBP):
+        v = cols["sorted_33009"]
+        if fmt == O.UNCOMPR:
+            s = ref.agg_sum(fmt, 0, v.view(np.uint8), (len(v), 8 * len(v), 0))
+        else:
+            b, m = ref.compress(fmt, 0, v)
+            s = ref.agg_sum(fmt, 0, b, m)
+        fx[f"agg_sum/{fmt}"] = np.array([s], dtype=np.uint64)
+    # --- semi_join ----------------------------------------------------------------------
+    dim = orc.sorted_gaps(5, orc.geom_table(0.25), 3000)
+    keep = orc.uniform_bits(6, 4, len(dim)) < 2
+    lkeys = dim[keep]
+    fk = orc.uniform_bits(7, 14, 30_011)
+    fx["semi/l"] = lkeys
+    fx["semi/r"] = fk
+    lb, lm = ref.compress(O.DELTA_DVBP, 0, lkeys)
+    rb, rm = ref.compress(O.FOR_DVBP, 0, fk)
+    for out_fmt in (O.UNCOMPR, O.DYNAMIC_VBP, O.DELTA_DVBP):
+        ob, om = ref.semi_join(O.DELTA_DVBP, lb, lm, O.FOR_DVBP, rb, rm, out_fmt)
+        fx[f"semi/{out_fmt}/bytes"] = O.mask_gap(out_fmt, 0, ob, om, orc)
+        fx[f"semi/{out_fmt}/meta"] = np.array(om, dtype=np.uint64)
+    # --- intersect -----------------------------------------------------------------------
+    a = np.flatnonzero(orc.uniform_bits(8, 3, 20_000) < 3).astype(np.uint64)
+    b2 = np.flatnonzero(orc.uniform_bits(9, 3, 20_000) < 5).astype(np.uint64)
+    fx["isect/l"], fx["isect/r"] = a, b2
+    ab, am = ref.compress(O.DYNAMIC_VBP, 0, a)
+    ob, om = ref.intersect(O.DYNAMIC_VBP, ab, am, b2, O.UNCOMPR)
+    fx["isect/out"] = ob.view(np.uint64)
+    # --- group + grouped sum ---------------------------------------------------------------
+    g = orc.from_table(10, orc.zipf_table(1.1, 1000), 50_003)
+    meas = orc.uniform_bits(11, 16, len(g))
+    fx["group/in"], fx["group/meas"] = g, meas
+    gb, gm = ref.compress(O.DYNAMIC_VBP, 0, g)
+    (grb, grm), (exb, exm) = ref.group(O.DYNAMIC_VBP, gb, gm, O.UNCOMPR, O.UNCOMPR)
+    fx["group/gr"] = grb.view(np.uint64)
+    fx["group/ext"] = exb.view(np.uint64)
+    (grb2, grm2), (exb2, exm2) = ref.group(O.DYNAMIC_VBP, gb, gm, O.DYNAMIC_VBP, O.DYNAMIC_VBP)
+    fx["group/gr_dvbp/bytes"] = O.mask_gap(O.DYNAMIC_VBP, 0, grb2, grm2, orc)
+    fx["group/gr_dvbp/meta"] = np.array(grm2, dtype=np.uint64)
+    fx["group/ext_dvbp/bytes"] = O.mask_gap(O.DYNAMIC_VBP, 0, exb2, exm2, orc)
+    fx["group/ext_dvbp/meta"] = np.array(exm2, dtype=np.uint64)
+    fx["group/sum"] = ref.agg_sum_grouped(fx["group/gr"], meas, len(fx["group/ext"]))
+    np.savez_compressed(OUT, **fx)
+    print(f"wrote {OUT}: {len(fx)} arrays, {os.path.getsize(OUT)} bytes")
+
+
+if __name__ == "__main__":
+    main()
