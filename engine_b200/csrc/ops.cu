@@ -5,6 +5,8 @@
 // decoded values in registers, so uncompressed data never round-trips
 // through HBM (the reference's decompress_and_process_batch, format.h:164-195,
 // weaves decoding into the operator the same way on the CPU).
+#include <mutex>
+
 #include "internal.h"
 #include "scan.cuh"
 
@@ -375,5 +377,113 @@ extern "C" int ms_gpu_select_project_sum_async(const ms_col *xc, int cmp, uint64
                                                                 (unsigned long long *)d_count, nullptr, d_err);
         MS_CUDA_TRY(cudaGetLastError());
     }
+    return MS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free select.
+//
+// Some callers cannot allocate device memory at all: code that runs after a
+// host application has reserved the whole device budget up front, engines
+// whose memory is owned by another allocator (a database buffer pool, a
+// plugin host), and paths where cudaMalloc / cudaFree are forbidden because
+// they synchronise the device.  For them this entry point takes the caller's
+// input and output buffers and keeps its own scratch (per-block hit counts,
+// block offsets, scan partials, two counters) in one file-scope device
+// array, kNoAllocScratchBytes large, which every GPU that loads the library
+// holds until the process exits.  Inputs are limited to kNoAllocMaxRows rows
+// so that the scratch fits.
+//
+// The array's host-side name is not a device address: its device address is
+// looked up with cudaGetSymbolAddress once per device, with that device
+// current, on the first call made on the device.  That first call should
+// therefore happen before any stream capture.  Every call shares the one
+// array and it keeps the last call's contents, so calls that overlap on the
+// GPU (concurrent streams, other threads) race; the counters that must start
+// at zero are cleared at the start of every call.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr uint64_t round256(uint64_t x) { return (x + 255) / 256 * 256; }
+constexpr uint64_t kNoAllocMaxRows = uint64_t(1) << 26;
+constexpr uint64_t kNoAllocMaxBlocks = kNoAllocMaxRows / kBlock;
+constexpr uint64_t kNoAllocCountsBytes = round256(4 * kNoAllocMaxBlocks);
+constexpr uint64_t kNoAllocOffsetsBytes = round256(8 * kNoAllocMaxBlocks);
+constexpr uint64_t kNoAllocScanWords = 2 * ((kNoAllocMaxBlocks + kScanTile - 1) / kScanTile) + 2 * 1 + 1;
+constexpr uint64_t kNoAllocScanBytes = round256(8 * kNoAllocScanWords);
+constexpr uint64_t kNoAllocWordsBytes = 256;  // scalar-hit counter, error word
+constexpr uint64_t kNoAllocScratchBytes =
+    kNoAllocCountsBytes + kNoAllocOffsetsBytes + kNoAllocScanBytes + kNoAllocWordsBytes;
+
+static_assert(kNoAllocScratchBytes <= (uint64_t(2) << 20), "no-alloc scratch is stated as at most 2 MiB");
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+}  // namespace
+
+static int noalloc_scratch_address(unsigned char **out) {
+    constexpr int kMaxDevices = 64;
+    static unsigned char *addr[kMaxDevices] = {};
+    static std::mutex mu;
+    int dev = 0;
+    MS_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return ms_fail(MS_ERR_INVALID, "select_noalloc: device ordinal out of range");
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[dev]) {
+        void *p = nullptr;
+        MS_CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        addr[dev] = static_cast<unsigned char *>(p);
+    }
+    *out = addr[dev];
+    return MS_OK;
+}
+
+extern "C" uint64_t ms_gpu_select_noalloc_max_rows(void) { return kNoAllocMaxRows; }
+
+extern "C" int ms_gpu_select_noalloc(int cmp, uint64_t val, const ms_col *in, uint64_t *d_out_pos,
+                                     uint64_t out_capacity, uint64_t *d_out_count, unsigned *d_err, void *stream) {
+    if (!in || !d_out_count || (!d_out_pos && in->count_values))
+        return ms_fail(MS_ERR_INVALID, "select_noalloc: null argument");
+    if (cmp < MS_CMP_EQ || cmp > MS_CMP_GE) return ms_fail(MS_ERR_INVALID, "select_noalloc: unknown comparison");
+    int rc = check_col(in, false);
+    if (rc) return rc;
+    if (in->count_values > kNoAllocMaxRows)
+        return ms_fail(MS_ERR_INVALID, "select_noalloc: column longer than 2^26 rows (the scratch limit)");
+    if (out_capacity < in->count_values)
+        return ms_fail(MS_ERR_INVALID, "select_noalloc: output capacity below the column length");
+    if (in->format == MS_FMT_RLE || in->format == MS_FMT_DELTA_DVBP)
+        return ms_fail(MS_ERR_UNSUPPORTED, "select_noalloc: rle_f / delta_f inputs need more scratch");
+    const uint64_t nb_compr = (in->count_values - count_rest(*in)) / kBlock;
+    if ((in->format == MS_FMT_DYNAMIC_VBP || in->format == MS_FMT_FOR_DVBP) && nb_compr &&
+        (!in->index || in->n_index < nb_compr || (in->format == MS_FMT_FOR_DVBP && !in->index_aux)))
+        return ms_fail(MS_ERR_INVALID, "select_noalloc: dynamic_vbp / for_f input needs its block index");
+    unsigned char *scr = nullptr;
+    rc = noalloc_scratch_address(&scr);
+    if (rc) return rc;
+    uint32_t *counts = reinterpret_cast<uint32_t *>(scr);
+    uint64_t *offsets = reinterpret_cast<uint64_t *>(scr + kNoAllocCountsBytes);
+    uint64_t *scan_scr = reinterpret_cast<uint64_t *>(scr + kNoAllocCountsBytes + kNoAllocOffsetsBytes);
+    unsigned long long *scalar_hits =
+        reinterpret_cast<unsigned long long *>(scr + kNoAllocCountsBytes + kNoAllocOffsetsBytes + kNoAllocScanBytes);
+    unsigned *own_err = reinterpret_cast<unsigned *>(scalar_hits + 1);
+    unsigned *err = d_err ? d_err : own_err;
+    cudaStream_t st = (cudaStream_t)stream;
+    ColView x;
+    rc = prepare_view(in, nullptr, st, &x);
+    if (rc) return rc;
+    MS_CUDA_TRY(cudaMemsetAsync(scalar_hits, 0, kNoAllocWordsBytes, st));
+    if (d_err) MS_CUDA_TRY(cudaMemsetAsync(d_err, 0, sizeof(unsigned), st));
+    const uint64_t nbt = x.nblocks_total();
+    if (nbt == 0) {
+        MS_CUDA_TRY(cudaMemsetAsync(d_out_count, 0, 8, st));
+        return MS_OK;
+    }
+    if (scan_scratch_words(nbt, 1) > kNoAllocScanWords)
+        return ms_fail(MS_ERR_INVALID, "select_noalloc: scan scratch too small");
+    const unsigned grid = grid_for_blocks(nbt);
+    k_sps<true, false><<<grid, 256, 0, st>>>(x, x, cmp, val, nullptr, nullptr, counts, err);
+    MS_CUDA_TRY(cudaGetLastError());
+    MS_CUDA_TRY((scan_exclusive<uint32_t, 1>(counts, nbt, offsets, d_out_count, scan_scr, st)));
+    k_select_write<false><<<grid, 256, 0, st>>>(x, x, cmp, val, offsets, d_out_pos, nullptr, scalar_hits, err);
+    MS_CUDA_TRY(cudaGetLastError());
     return MS_OK;
 }

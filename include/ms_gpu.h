@@ -179,6 +179,25 @@ int ms_gpu_group(const ms_col *gr_in, const ms_col *in, int gr_format, ms_col *o
 int ms_gpu_agg_sum_grouped(const ms_col *gr, const ms_col *data, uint64_t n_groups,
                            ms_col *out, ms_arena *arena, void *stream);
 
+/* Allocation-free select (no counterpart in the reference).  For callers that
+ * cannot allocate device memory -- the device budget was reserved up front by
+ * the host application, memory belongs to another allocator (a buffer pool, a
+ * plugin host), or cudaMalloc/cudaFree must be avoided because they
+ * synchronise the device.  The caller passes the input column and the output
+ * buffers: d_out_pos (capacity out_capacity >= count_values; uncompressed
+ * ascending positions) and d_out_count (the hit count, device memory);
+ * d_err (optional, device) receives kernel error bits.  Nothing is allocated:
+ * scratch lives in a 2 MiB file-scope device array that every GPU loading the
+ * library keeps until exit, so inputs are limited to
+ * ms_gpu_select_noalloc_max_rows() = 2^26 rows; longer inputs, delta_f/rle_f
+ * inputs and dynamic_vbp/for_f inputs without a block index are rejected.
+ * The first call on a device looks up the array's device address, so make it
+ * before any stream capture.  All calls share the array and it keeps the last
+ * call's contents: calls that overlap on the GPU race.  Asynchronous. */
+int ms_gpu_select_noalloc(int cmp, uint64_t val, const ms_col *in, uint64_t *d_out_pos,
+                          uint64_t out_capacity, uint64_t *d_out_count, unsigned *d_err, void *stream);
+uint64_t ms_gpu_select_noalloc_max_rows(void);
+
 /* ---- synthetic data (device-side, counter-based splitmix64) -------------- */
 int ms_gpu_gen_uniform_bits(uint64_t seed, unsigned bits, uint64_t n, uint64_t *d_out, void *stream);
 int ms_gpu_gen_from_table(uint64_t seed, const uint64_t *d_table, uint64_t n_table, uint64_t n,
