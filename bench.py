@@ -234,6 +234,8 @@ def run_gpu(args):
     ms._check(lib.ms_gpu_morph(C.byref(ux), ms.DYNAMIC_VBP, 0, C.byref(xc), arena.h, sp), "morph x")
     ms._check(lib.ms_gpu_morph(C.byref(uy), ms.DYNAMIC_VBP, 0, C.byref(yc), arena.h, sp), "morph y")
     algo_bytes = int(xc.size_used_byte) + int(yc.size_used_byte) + 8
+    from engine_b200 import autotune
+    tuned = autotune.apply(ms, xc, yc)
 
     # expected result (device-side check with torch on the uncompressed inputs)
     tx = ms._device_view(xu, 8 * n).view(torch.int64)
@@ -296,11 +298,12 @@ def run_gpu(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "rows_per_gpu": n, "compressed_bytes_per_gpu": algo_bytes,
                        "parallelism": f"replicas{world}" if world > 1 else "single",
-                       "l2": "inputs (1.0 GB) larger than L2; no flush"},
+                       "l2": "inputs (1.0 GB) larger than L2; no flush",
+                       "launch": dict(ms.get_tuning(), source="tuning.json" if tuned else "default")},
             "parity": {"sum_ok": ok, "count": got_cnt},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "peak_source": peak_kind,
-                         "traffic": _traffic_per_launch(), "kernel": "k_sps<true,true> (ops.cu)",
+                         "traffic": _traffic_per_launch(), "kernel": "k_sps_tma (sps_tma.cu)" if ms.get_tuning()["staged"] else "k_sps (ops.cu)",
                          "algorithmic_bytes_per_launch": algo_bytes},
             "clocks": clk.summary(), "e2e": e2e, "gpu_launches": args.steps}
     if rank == 0 and world == 1 and not args.no_cpu:

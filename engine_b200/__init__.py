@@ -43,6 +43,11 @@ class MorphStoreError(RuntimeError):
         self.status = status
 
 
+class MsTuning(C.Structure):
+    _fields_ = [("staged", C.c_int), ("warps", C.c_uint), ("stages", C.c_uint), ("stage_bytes", C.c_uint),
+                ("ctas_per_sm", C.c_uint)]
+
+
 class MsCol(C.Structure):
     _fields_ = [("format", C.c_uint32), ("bw", C.c_uint32), ("count_values", C.c_uint64),
                 ("size_used_byte", C.c_uint64), ("size_compr_byte", C.c_uint64),
@@ -77,6 +82,8 @@ _sig = {
     "ms_gpu_intersect_sorted": (C.c_int, [_P(MsCol), _P(MsCol), C.c_int, C.c_uint, _P(MsCol), _V, _V]),
     "ms_gpu_group": (C.c_int, [_P(MsCol), _P(MsCol), C.c_int, _P(MsCol), C.c_int, _P(MsCol), _V, _V]),
     "ms_gpu_agg_sum_grouped": (C.c_int, [_P(MsCol), _P(MsCol), _U64, _P(MsCol), _V, _V]),
+    "ms_gpu_set_tuning": (C.c_int, [_P(MsTuning)]),
+    "ms_gpu_get_tuning": (C.c_int, [_P(MsTuning)]),
     "ms_gpu_gen_uniform_bits": (C.c_int, [_U64, C.c_uint, _U64, _V, _V]),
     "ms_gpu_gen_from_table": (C.c_int, [_U64, _V, _U64, _U64, _V, _V]),
 }
@@ -419,6 +426,19 @@ def agg_sum_grouped(gr: Column, data: Column, n_groups: int, stream=None) -> Col
     _check(_lib.ms_gpu_agg_sum_grouped(C.byref(gr.desc), C.byref(data.desc), n_groups, C.byref(out), gr.arena.h,
                                        _stream_ptr(stream)), "agg_sum_grouped")
     return Column(out, gr.arena, keep=(gr, data))
+
+
+def set_tuning(staged: int = 1, warps: int = 8, stages: int = 8, stage_bytes: int = 24576,
+               ctas_per_sm: int = 1) -> None:
+    """Launch parameters of the fused kernels (ms_gpu_set_tuning)."""
+    t = MsTuning(staged, warps, stages, stage_bytes, ctas_per_sm)
+    _check(_lib.ms_gpu_set_tuning(C.byref(t)), "set_tuning")
+
+
+def get_tuning() -> dict:
+    t = MsTuning()
+    _check(_lib.ms_gpu_get_tuning(C.byref(t)), "get_tuning")
+    return {k: getattr(t, k) for k, _ in MsTuning._fields_}
 
 
 def device_info():

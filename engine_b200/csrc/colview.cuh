@@ -32,6 +32,31 @@ struct ColView {
     __host__ __device__ uint64_t nblocks_total() const { return (n + kBlock - 1) / kBlock; }
 };
 
+// Cascade step after unpacking block b of the compressed part: for_f adds
+// the 1024-block reference (for.h:385-467); delta_f turns the deltas into
+// values with a lane-wise running sum -- thread-local over its 16 slots,
+// across the four quarters of the lane by shuffles, plus the block's
+// carry-in (delta.h:285-347).
+__device__ __forceinline__ void apply_cascade(const ColView &c, uint64_t b, unsigned l, unsigned q,
+                                              uint64_t (&v)[16]) {
+    if (c.fmt == MS_FMT_FOR_DVBP) {
+        const uint64_t ref = __ldg(c.aux + (b >> 1));
+#pragma unroll
+        for (int k = 0; k < 16; k++) v[k] += ref;
+    } else if (c.fmt == MS_FMT_DELTA_DVBP) {
+#pragma unroll
+        for (int k = 1; k < 16; k++) v[k] += v[k - 1];
+        const uint64_t tot = v[15];
+        const uint64_t up = __shfl_up_sync(0xFFFFFFFFu, tot, 8);
+        uint64_t pre = q >= 1 ? up : 0;
+        const uint64_t up2 = __shfl_up_sync(0xFFFFFFFFu, tot + pre, 16);
+        pre += q >= 2 ? up2 : 0;
+        pre += __ldg(c.carry + b * 8 + l);
+#pragma unroll
+        for (int k = 0; k < 16; k++) v[k] += pre;
+    }
+}
+
 // Decode rows of block b for thread (l, q): v[k] = row b*512 + (16q+k)*8 + l.
 // Rows >= n are returned as 0; `valid` gets bit k set for rows < n.
 // Returns false (and sets *err) for a corrupt bit width.
@@ -51,25 +76,7 @@ __device__ __forceinline__ bool decode_block(const ColView &c, uint64_t b, unsig
             bw = idx_bw(e);
         }
         const bool ok = vbp_decode16_rt(bw, reinterpret_cast<const uint64_t *>(c.data + off), l, q, v);
-        if (c.fmt == MS_FMT_FOR_DVBP) {
-            const uint64_t ref = __ldg(c.aux + (b >> 1));
-#pragma unroll
-            for (int k = 0; k < 16; k++) v[k] += ref;
-        } else if (c.fmt == MS_FMT_DELTA_DVBP) {
-            // lane-wise running sum: thread-local prefix over its 16 slots,
-            // then across the four quarters of the same lane, plus carry-in.
-#pragma unroll
-            for (int k = 1; k < 16; k++) v[k] += v[k - 1];
-            uint64_t tot = v[15];
-            uint64_t up = __shfl_up_sync(0xFFFFFFFFu, tot, 8);
-            uint64_t pre = q >= 1 ? up : 0;
-            uint64_t t2 = tot + pre;
-            uint64_t up2 = __shfl_up_sync(0xFFFFFFFFu, t2, 16);
-            pre += q >= 2 ? up2 : 0;
-            pre += __ldg(c.carry + b * 8 + l);
-#pragma unroll
-            for (int k = 0; k < 16; k++) v[k] += pre;
-        }
+        apply_cascade(c, b, l, q, v);
         return ok;
     }
     // uncompressed rows

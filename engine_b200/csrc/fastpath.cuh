@@ -1,0 +1,164 @@
+// fastpath.cuh -- predicate and sum evaluated inside the bit-width switch.
+//
+// For plain vbp blocks (static_vbp, dynamic_vbp, uncompressed viewed as
+// vbp_l<64,8>) the value range of a block is known at compile time inside
+// each switch case: values of a bw-bit block are < 2^bw.  The select
+// predicate therefore reduces to one unsigned threshold test, and for
+// bw <= 32 decoding, comparing and summing run on 32-bit registers (one
+// funnel shift + one mask per value) instead of 64-bit pairs.
+//
+// Predicate reduction (values v < 2^63, compared as signed 64-bit integers
+// as the reference's AVX-512 primitives do, compare_avx512.h:35-111):
+//   less c      : v <  T, T = c if (int64)c > 0 else 0
+//   lessequal c : v <  T, T = c+1 if (int64)c >= 0 else 0
+//   greater c   : !(v < T) with T of lessequal;  greaterequal: !(v < T) of less
+//   equal c     : v == c
+// 64-bit blocks (values may reach 2^63) use the signed compare directly.
+#pragma once
+
+#include "colview.cuh"
+
+namespace ms {
+
+struct Pred {
+    int cmp;        // original comparison (64-bit blocks)
+    uint64_t val;   // original constant
+    int is_eq;      // equal
+    uint64_t T;     // threshold (v < T), in [0, 2^63]
+    int flip;       // negate the threshold test
+};
+
+inline Pred make_pred(int cmp, uint64_t c) {
+    Pred p{cmp, c, cmp == MS_CMP_EQ, 0, 0};
+    const int64_t cs = (int64_t)c;
+    switch (cmp) {
+    case MS_CMP_LT: p.T = cs > 0 ? c : 0; break;
+    case MS_CMP_LE: p.T = cs >= 0 ? c + 1 : 0; break;
+    case MS_CMP_GT: p.T = cs >= 0 ? c + 1 : 0; p.flip = 1; break;
+    case MS_CMP_GE: p.T = cs > 0 ? c : 0; p.flip = 1; break;
+    default: break;
+    }
+    return p;
+}
+
+// 16 values of quarter q of lane l as 32-bit integers (bw <= 32).
+template <unsigned BW>
+__device__ __forceinline__ void vbp_decode16_u32(const uint64_t *__restrict__ blk, unsigned l, unsigned q,
+                                                 uint32_t (&v)[16]) {
+    static_assert(BW <= 32, "32-bit decode");
+    constexpr unsigned NW = (16 * BW + 63) / 64 + 1;  // 64-bit words covering the quarter (+1 for the shift)
+    constexpr unsigned NH = (16 * BW + 31) / 32 + 1;  // 32-bit words after normalisation (+1 spare)
+    const unsigned sbit = 16u * q * BW;
+    const unsigned w0 = sbit >> 6;
+    uint32_t h[2 * NW];
+#pragma unroll
+    for (unsigned i = 0; i < NW; i++) {
+        const uint64_t w = (w0 + i < BW) ? blk[(w0 + i) * 8 + l] : 0;
+        h[2 * i] = uint32_t(w);
+        h[2 * i + 1] = uint32_t(w >> 32);
+    }
+    // start inside the loaded words: o whole 32-bit words, then t bits (0 or 16)
+    const unsigned o = (sbit >> 5) & 1u;
+    const unsigned t = sbit & 31u;
+    uint32_t n[NH];
+#pragma unroll
+    for (unsigned i = 0; i < NH; i++) {
+        const uint32_t a = (i + 1 < 2 * NW) ? (o ? h[i + 1] : h[i]) : 0;
+        const uint32_t b = (i + 2 < 2 * NW) ? (o ? h[i + 2] : h[i + 1]) : ((i + 1 < 2 * NW && !o) ? h[i + 1] : 0);
+        n[i] = (BW % 2 == 0) ? a : __funnelshift_r(a, b, t);
+    }
+    constexpr uint32_t M = BW == 32 ? 0xFFFFFFFFu : ((1u << BW) - 1u);
+#pragma unroll
+    for (unsigned k = 0; k < 16; k++) {
+        const unsigned p = k * BW, wi = p >> 5, sh = p & 31u;
+        uint32_t x = (sh + BW <= 32) ? (n[wi] >> sh) : __funnelshift_r(n[wi], n[wi + 1], sh);
+        v[k] = x & M;
+    }
+}
+
+template <unsigned BW>
+__device__ __forceinline__ unsigned mask_block(const uint64_t *blk, unsigned l, unsigned q, const Pred &p) {
+    unsigned m = 0;
+    if (BW <= 32) {
+        uint32_t v[16];
+        vbp_decode16_u32<(BW <= 32 ? BW : 32)>(blk, l, q, v);
+        if (p.is_eq) {
+            const bool in = p.val < (uint64_t(1) << 32);
+            const uint32_t c = uint32_t(p.val);
+#pragma unroll
+            for (int k = 0; k < 16; k++) m |= unsigned(in && v[k] == c) << k;
+        } else {
+            const bool big = p.T > 0xFFFFFFFFull;  // every value is below T
+            const uint32_t T = uint32_t(p.T);
+#pragma unroll
+            for (int k = 0; k < 16; k++) m |= unsigned(big || v[k] < T) << k;
+            if (p.flip) m ^= 0xFFFFu;
+        }
+    } else {
+        uint64_t v[16];
+        vbp_decode16<BW, true>(blk, l, q, v);
+        if (BW == 64) {
+#pragma unroll
+            for (int k = 0; k < 16; k++) m |= unsigned(cmp_eval(p.cmp, v[k], p.val, true)) << k;
+        } else if (p.is_eq) {
+#pragma unroll
+            for (int k = 0; k < 16; k++) m |= unsigned(v[k] == p.val) << k;
+        } else {
+#pragma unroll
+            for (int k = 0; k < 16; k++) m |= unsigned(v[k] < p.T) << k;
+            if (p.flip) m ^= 0xFFFFu;
+        }
+    }
+    return m;
+}
+
+template <unsigned BW>
+__device__ __forceinline__ uint64_t sum_block(const uint64_t *blk, unsigned l, unsigned q, unsigned m) {
+    if (BW <= 27) {  // 16 values of < 2^27 fit a 32-bit partial sum
+        uint32_t v[16];
+        vbp_decode16_u32<(BW <= 27 ? BW : 27)>(blk, l, q, v);
+        uint32_t s = 0;
+#pragma unroll
+        for (int k = 0; k < 16; k++) s += ((m >> k) & 1u) ? v[k] : 0u;
+        return s;
+    } else {
+        uint64_t v[16];
+        vbp_decode16<BW, true>(blk, l, q, v);
+        uint64_t s = 0;
+#pragma unroll
+        for (int k = 0; k < 16; k++) s += ((m >> k) & 1u) ? v[k] : 0;
+        return s;
+    }
+}
+
+#define MS_BW_CASES(X)                                                                                  \
+    X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16) X(17) X(18) \
+    X(19) X(20) X(21) X(22) X(23) X(24) X(25) X(26) X(27) X(28) X(29) X(30) X(31) X(32) X(33) X(34)   \
+    X(35) X(36) X(37) X(38) X(39) X(40) X(41) X(42) X(43) X(44) X(45) X(46) X(47) X(48) X(49) X(50)   \
+    X(51) X(52) X(53) X(54) X(55) X(56) X(57) X(58) X(59) X(60) X(61) X(62) X(63) X(64)
+
+// Hit mask of a plain vbp block (bit k = row (16q+k)*8+l); bw 0 or > 64
+// sets *bad.
+__device__ __forceinline__ unsigned mask_block_rt(unsigned bw, const uint64_t *blk, unsigned l, unsigned q,
+                                                  const Pred &p, bool &bad) {
+    switch (bw) {
+#define MS_X(B) \
+    case B: return mask_block<B>(blk, l, q, p);
+        MS_BW_CASES(MS_X)
+#undef MS_X
+    default: bad = true; return 0;
+    }
+}
+
+__device__ __forceinline__ uint64_t sum_block_rt(unsigned bw, const uint64_t *blk, unsigned l, unsigned q,
+                                                 unsigned m, bool &bad) {
+    switch (bw) {
+#define MS_X(B) \
+    case B: return sum_block<B>(blk, l, q, m);
+        MS_BW_CASES(MS_X)
+#undef MS_X
+    default: bad = true; return 0;
+    }
+}
+
+}  // namespace ms

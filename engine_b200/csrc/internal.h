@@ -57,4 +57,12 @@ int decompress_to(const ms_col *in, uint64_t *d_out, ms_arena *a, cudaStream_t s
 
 int read_err(ms_arena *a, cudaStream_t st);
 
+// Current launch parameters of the fused kernels (ms_gpu_set_tuning).
+ms_tuning tuning();
+
+// Staged (TMA) fused select/sum: see sps_tma.cu.
+int sps_tma(const ColView &x, const ColView &y, bool has_y, int cmp, uint64_t val, unsigned warps, unsigned stages,
+            unsigned stage_bytes, unsigned ctas_per_sm, uint64_t *d_sum, uint64_t *d_cnt, unsigned *d_err,
+            cudaStream_t st);
+
 }  // namespace ms

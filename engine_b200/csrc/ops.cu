@@ -243,6 +243,23 @@ int gather_values(const ms_col *data, const uint64_t *d_pos, uint64_t npos, uint
 
 using namespace ms;
 
+// The fused select/sum launch: staged (TMA) pipeline or direct loads, as
+// the current tuning says.
+static int launch_sps(const ColView &x, const ColView &y, int cmp, uint64_t c, uint64_t *d_sum, uint64_t *d_count,
+                      unsigned *d_err, cudaStream_t st) {
+    MS_CUDA_TRY(cudaMemsetAsync(d_sum, 0, 8, st));
+    if (d_count) MS_CUDA_TRY(cudaMemsetAsync(d_count, 0, 8, st));
+    const uint64_t nbt = x.nblocks_total();
+    if (!nbt) return MS_OK;
+    const ms_tuning t = tuning();
+    if (t.staged)
+        return sps_tma(x, y, true, cmp, c, t.warps, t.stages, t.stage_bytes, t.ctas_per_sm, d_sum, d_count, d_err, st);
+    k_sps<true, true><<<grid_for_blocks(nbt), 256, 0, st>>>(x, y, cmp, c, (unsigned long long *)d_sum,
+                                                            (unsigned long long *)d_count, nullptr, d_err);
+    MS_CUDA_TRY(cudaGetLastError());
+    return MS_OK;
+}
+
 extern "C" int ms_gpu_agg_sum(const ms_col *in, uint64_t *d_sum, ms_arena *a, void *stream) {
     if (!in || !d_sum || !a) return ms_fail(MS_ERR_INVALID, "agg_sum: null argument");
     int rc = check_col(in, false);
@@ -331,14 +348,8 @@ extern "C" int ms_gpu_select_project_sum(const ms_col *xc, int cmp, uint64_t c, 
     if (rc) return rc;
     rc = prepare_view(yc, a, st, &y);
     if (rc) return rc;
-    MS_CUDA_TRY(cudaMemsetAsync(d_sum, 0, 8, st));
-    if (d_count) MS_CUDA_TRY(cudaMemsetAsync(d_count, 0, 8, st));
-    const uint64_t nbt = x.nblocks_total();
-    if (nbt) {
-        k_sps<true, true><<<grid_for_blocks(nbt), 256, 0, st>>>(x, y, cmp, c, (unsigned long long *)d_sum,
-                                                                (unsigned long long *)d_count, nullptr, a->d_err);
-        MS_CUDA_TRY(cudaGetLastError());
-    }
+    rc = launch_sps(x, y, cmp, c, d_sum, d_count, a->d_err, st);
+    if (rc) return rc;
     if (d_pos || d_vals) {
         uint64_t *pos, *vals, cnt, nscal;
         rc = select_positions(x, &y, cmp, c, a, st, &pos, &vals, &cnt, &nscal);
@@ -369,15 +380,7 @@ extern "C" int ms_gpu_select_project_sum_async(const ms_col *xc, int cmp, uint64
     if (rc) return rc;
     rc = prepare_view(yc, nullptr, st, &y);
     if (rc) return rc;
-    MS_CUDA_TRY(cudaMemsetAsync(d_sum, 0, 8, st));
-    if (d_count) MS_CUDA_TRY(cudaMemsetAsync(d_count, 0, 8, st));
-    const uint64_t nbt = x.nblocks_total();
-    if (nbt) {
-        k_sps<true, true><<<grid_for_blocks(nbt), 256, 0, st>>>(x, y, cmp, c, (unsigned long long *)d_sum,
-                                                                (unsigned long long *)d_count, nullptr, d_err);
-        MS_CUDA_TRY(cudaGetLastError());
-    }
-    return MS_OK;
+    return launch_sps(x, y, cmp, c, d_sum, d_count, d_err, st);
 }
 
 // ---------------------------------------------------------------------------

@@ -20,6 +20,29 @@ int ms_fail(int status, const char *what) {
 
 extern "C" int ms_gpu_abi_version(void) { return MS_ABI_VERSION; }
 
+static ms_tuning g_tuning = {1, 8, 8, 24576, 1};
+
+ms_tuning ms::tuning() { return g_tuning; }
+
+extern "C" int ms_gpu_set_tuning(const ms_tuning *t) {
+    if (!t) return ms_fail(MS_ERR_INVALID, "set_tuning: null");
+    if (t->staged) {
+        if (t->warps != 4 && t->warps != 8 && t->warps != 12 && t->warps != 16 && t->warps != 24)
+            return ms_fail(MS_ERR_INVALID, "set_tuning: warps must be 4, 8, 12, 16 or 24");
+        if (t->stages < 2 || t->stages > 32 || t->stage_bytes < 8320 || t->stage_bytes % 128 ||
+            uint64_t(t->stages) * t->stage_bytes > 220 * 1024 || t->ctas_per_sm < 1 || t->ctas_per_sm > 4)
+            return ms_fail(MS_ERR_INVALID, "set_tuning: stages x stage_bytes must fit shared memory");
+    }
+    g_tuning = *t;
+    return MS_OK;
+}
+
+extern "C" int ms_gpu_get_tuning(ms_tuning *t) {
+    if (!t) return ms_fail(MS_ERR_INVALID, "get_tuning: null");
+    *t = g_tuning;
+    return MS_OK;
+}
+
 extern "C" const char *ms_gpu_status_string(int status) {
     static const char *names[] = {"MS_OK",          "MS_ERR_INVALID", "MS_ERR_UNSUPPORTED", "MS_ERR_CUDA",
                                   "MS_ERR_NOMEM",   "MS_ERR_CORRUPT", "MS_ERR_TIMEOUT"};

@@ -102,6 +102,21 @@ int ms_gpu_arena_check(ms_arena *a, void *stream);
 int ms_gpu_memcpy(void *dst, const void *src, uint64_t bytes, int kind, int sync, void *stream);
 int ms_gpu_stream_sync(void *stream);
 
+/* Launch parameters of the fused kernels, chosen per format class by the
+ * autotuner (engine_b200/autotune.py) or set by hand.  staged = 1 selects the
+ * TMA-staged pipeline (shared-memory ring of `stages` x `stage_bytes` per CTA,
+ * `warps` consumer warps, `ctas_per_sm` CTAs per SM); 0 the direct-load
+ * kernel (one warp per 512-row block, loads straight from HBM). */
+typedef struct ms_tuning {
+    int staged;
+    unsigned warps;
+    unsigned stages;
+    unsigned stage_bytes;
+    unsigned ctas_per_sm;
+} ms_tuning;
+int ms_gpu_set_tuning(const ms_tuning *t);
+int ms_gpu_get_tuning(ms_tuning *t);
+
 /* ---- layout arithmetic (host only) --------------------------------------- */
 /* get_size_max_byte_any_len<F>(n)  (include/core/morphing/format.h:114-153) */
 uint64_t ms_size_max_byte_any_len(int format, unsigned bw, uint64_t count_values);

@@ -278,6 +278,8 @@ class Reference:
         L.ref_agg_sum.argtypes = [C.c_int, C.c_uint, U8P, M, U64P]
         L.ref_semi_join.argtypes = [C.c_int, U8P, M, C.c_int, U8P, M, C.c_int, U8P, C.c_uint64, M]
         L.ref_intersect.argtypes = [C.c_int, U8P, M, U64P, C.c_uint64, C.c_int, U8P, C.c_uint64, M]
+        L.ref_intersect_scalar.restype = C.c_uint64
+        L.ref_intersect_scalar.argtypes = [U64P, C.c_uint64, U64P, C.c_uint64, U64P]
         L.ref_group.argtypes = [C.c_int, U8P, M, C.c_int, U8P, C.c_uint64, M, C.c_int, U8P, C.c_uint64, M]
         L.ref_agg_sum_grouped.argtypes = [U64P, U64P, C.c_uint64, C.c_uint64, U64P]
         L.ref_bench_select_project_sum.restype = C.c_uint64
@@ -370,6 +372,14 @@ class Reference:
             raise ValueError(f"ref_intersect rc={rc}")
         return out[: mo.size_used_byte].copy(), mo.tuple()
 
+    def intersect_scalar(self, l, r):
+        """scalar intersect_sorted (scalar/intersect_uncompr.h:41-86)."""
+        l, lp = _u64(l)
+        r, rp = _u64(r)
+        out = np.zeros(max(min(len(l), len(r)), 1), dtype=np.uint64)
+        k = self.lib.ref_intersect_scalar(lp, len(l), rp, len(r), out.ctypes.data_as(U64P))
+        return out[:k].copy()
+
     def group(self, in_fmt, data, meta, gr_fmt, ext_fmt):
         d = self._padded(data)
         cap = self._cap(meta[0])
@@ -416,11 +426,12 @@ def _mask_for_headers(d: np.ndarray, compr: int) -> None:
     """Walk the for_f pages and zero header words after a UINT64_MAX marker."""
     i = 0
     while i < compr:
-        hdr = d[i: i + 64].view(np.uint64)
+        h0 = i
+        hdr = d[i: i + 64].view(np.uint64).copy()
         i += 64
         for j in range(8):
             if int(hdr[j]) == 0xFFFFFFFFFFFFFFFF:
-                d[i - 64 + 8 * (j + 1): i] = 0
+                d[h0 + 8 * (j + 1): h0 + 64] = 0
                 break
             # inner dvbp page of one 1024-block: 64-B header + two packed blocks
             bws = d[i: i + 2]

@@ -22,7 +22,10 @@
 #include <core/operators/general_vectorized/join_semi_equi_compr.h>
 #include <core/operators/general_vectorized/intersect_compr.h>
 #include <core/operators/interfaces/join.h>
+#if defined(PART_OPS)
+// defines non-inline specialisations: one translation unit only
 #include <core/operators/scalar/agg_sum_uncompr.h>
+#endif
 #include <core/storage/column.h>
 #include <vector/vector_primitives.h>
 
