@@ -223,7 +223,7 @@ def run_gpu(args):
     arena = ms.Arena(16 << 30)
 
     # --- data: generated and compressed on the device (outside timing) -------
-    n = N_ROWS
+    n = 1 << args.log2_rows
     xu = arena.alloc(8 * n)
     yu = arena.alloc(8 * n)
     ms._check(lib.ms_gpu_gen_uniform_bits(SEED_X + rank, X_BITS, n, xu, sp), "gen x")
@@ -289,7 +289,7 @@ def run_gpu(args):
     value = world * algo_bytes / (ms_per_step * 1e-3) / 1e9
 
     # --- e2e: host buffers through the public API ----------------------------
-    e2e = e2e_run(ms, lib, arena, xc, yc, sp, args, exp_sum)
+    e2e = None if args.no_e2e else e2e_run(ms, lib, arena, xc, yc, sp, args, exp_sum)
 
     peak, peak_kind = _peaks()
     achieved = algo_bytes / (kern_ms * 1e-3) / 1e9
@@ -306,6 +306,8 @@ def run_gpu(args):
                          "traffic": _traffic_per_launch(), "kernel": "k_sps_tma (sps_tma.cu)" if ms.get_tuning()["staged"] else "k_sps (ops.cu)",
                          "algorithmic_bytes_per_launch": algo_bytes},
             "clocks": clk.summary(), "e2e": e2e, "gpu_launches": args.steps}
+    if args.log2_rows != 28:
+        line["config"]["note"] = "reduced size: profiling run, not the benchmark workload"
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
             line["cpu_baseline"] = cpu_baseline(1)
@@ -381,6 +383,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffer) leg")
+    ap.add_argument("--log2-rows", type=int, default=28, help="rows per GPU = 2^N (profiling runs use less)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -45,7 +45,7 @@ class MorphStoreError(RuntimeError):
 
 class MsTuning(C.Structure):
     _fields_ = [("staged", C.c_int), ("warps", C.c_uint), ("stages", C.c_uint), ("stage_bytes", C.c_uint),
-                ("ctas_per_sm", C.c_uint)]
+                ("ctas_per_sm", C.c_uint), ("values_per_thread", C.c_uint)]
 
 
 class MsCol(C.Structure):
@@ -428,10 +428,10 @@ def agg_sum_grouped(gr: Column, data: Column, n_groups: int, stream=None) -> Col
     return Column(out, gr.arena, keep=(gr, data))
 
 
-def set_tuning(staged: int = 1, warps: int = 8, stages: int = 8, stage_bytes: int = 24576,
-               ctas_per_sm: int = 1) -> None:
+def set_tuning(staged: int = 1, warps: int = 24, stages: int = 4, stage_bytes: int = 49152,
+               ctas_per_sm: int = 1, values_per_thread: int = 16) -> None:
     """Launch parameters of the fused kernels (ms_gpu_set_tuning)."""
-    t = MsTuning(staged, warps, stages, stage_bytes, ctas_per_sm)
+    t = MsTuning(staged, warps, stages, stage_bytes, ctas_per_sm, values_per_thread)
     _check(_lib.ms_gpu_set_tuning(C.byref(t)), "set_tuning")
 
 

@@ -21,9 +21,9 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CACHE = os.path.join(HERE, "tuning.json")
 
-CANDIDATES = [dict(staged=0, warps=8, stages=8, stage_bytes=24576, ctas_per_sm=1)] + [
-    dict(staged=1, warps=w, stages=s, stage_bytes=b, ctas_per_sm=1)
-    for w, s, b in itertools.product((8, 12, 16, 24), (3, 4, 6, 8), (16384, 24576, 32768, 49152))
+CANDIDATES = [dict(staged=0, warps=8, stages=8, stage_bytes=24576, ctas_per_sm=1, values_per_thread=16)] + [
+    dict(staged=1, warps=w, stages=s, stage_bytes=b, ctas_per_sm=1, values_per_thread=v)
+    for v, w, s, b in itertools.product((16, 32), (12, 16, 24), (3, 4, 6), (24576, 32768, 49152, 65536))
     if s * b <= 200 * 1024
 ]
 
@@ -96,7 +96,8 @@ def apply(ms, xc, yc) -> bool:
     entry = load_cache().get(key(xc, yc, ms.device_info()[0]))
     if not entry:
         return False
-    ms.set_tuning(**{k: entry[k] for k in ("staged", "warps", "stages", "stage_bytes", "ctas_per_sm")})
+    ms.set_tuning(**{k: entry[k] for k in ("staged", "warps", "stages", "stage_bytes", "ctas_per_sm",
+                                            "values_per_thread") if k in entry})
     return True
 
 

@@ -162,3 +162,104 @@ __device__ __forceinline__ uint64_t sum_block_rt(unsigned bw, const uint64_t *bl
 }
 
 }  // namespace ms
+
+namespace ms {
+
+// ---------------------------------------------------------------------------
+// 32 values per thread: thread (l, h) of a half-warp decodes slots 32h..32h+31
+// of lane l, i.e. rows (32h + k) * 8 + l.  The half starts at bit 32*h*bw,
+// always on a 32-bit word boundary, so even widths need no realignment and
+// odd widths only a word select.
+// ---------------------------------------------------------------------------
+template <unsigned BW>
+__device__ __forceinline__ void vbp_decode32_u32(const uint64_t *__restrict__ blk, unsigned l, unsigned h,
+                                                 uint32_t (&v)[32]) {
+    static_assert(BW <= 32, "32-bit decode");
+    constexpr unsigned NW = (32 * BW + 63) / 64 + 1;
+    constexpr unsigned NH = BW + 1;
+    const unsigned sbit = 32u * h * BW;
+    const unsigned w0 = sbit >> 6;
+    uint32_t hw[2 * NW];
+#pragma unroll
+    for (unsigned i = 0; i < NW; i++) {
+        const uint64_t w = (w0 + i < BW) ? blk[(w0 + i) * 8 + l] : 0;
+        hw[2 * i] = uint32_t(w);
+        hw[2 * i + 1] = uint32_t(w >> 32);
+    }
+    const unsigned o = (sbit >> 5) & 1u;  // 0 for even widths
+    uint32_t n[NH];
+#pragma unroll
+    for (unsigned i = 0; i < NH; i++) {
+        if (BW % 2 == 0) n[i] = (i < 2 * NW) ? hw[i] : 0;
+        else n[i] = (i + 1 < 2 * NW) ? (o ? hw[i + 1] : hw[i]) : ((i < 2 * NW && !o) ? hw[i] : 0);
+    }
+    constexpr uint32_t M = BW == 32 ? 0xFFFFFFFFu : ((1u << BW) - 1u);
+#pragma unroll
+    for (unsigned k = 0; k < 32; k++) {
+        const unsigned p = k * BW, wi = p >> 5, sh = p & 31u;
+        const uint32_t x = (sh + BW <= 32) ? (n[wi] >> sh) : __funnelshift_r(n[wi], n[wi + 1], sh);
+        v[k] = x & M;
+    }
+}
+
+template <unsigned BW>
+__device__ __forceinline__ unsigned mask32_block(const uint64_t *blk, unsigned l, unsigned h, const Pred &p) {
+    unsigned m = 0;
+    if (BW <= 32) {
+        uint32_t v[32];
+        vbp_decode32_u32<(BW <= 32 ? BW : 32)>(blk, l, h, v);
+        if (p.is_eq) {
+            const bool in = p.val < (uint64_t(1) << 32);
+            const uint32_t c = uint32_t(p.val);
+#pragma unroll
+            for (int k = 0; k < 32; k++) m |= unsigned(in && v[k] == c) << k;
+        } else {
+            const bool big = p.T > 0xFFFFFFFFull;
+            const uint32_t T = uint32_t(p.T);
+#pragma unroll
+            for (int k = 0; k < 32; k++) m |= unsigned(big || v[k] < T) << k;
+            if (p.flip) m = ~m;
+        }
+    } else {
+        m = mask_block<BW>(blk, l, 2 * h, p) | (mask_block<BW>(blk, l, 2 * h + 1, p) << 16);
+    }
+    return m;
+}
+
+template <unsigned BW>
+__device__ __forceinline__ uint64_t sum32_block(const uint64_t *blk, unsigned l, unsigned h, unsigned m) {
+    if (BW <= 26) {  // 32 values of < 2^26 fit a 32-bit partial sum
+        uint32_t v[32];
+        vbp_decode32_u32<(BW <= 26 ? BW : 26)>(blk, l, h, v);
+        uint32_t s = 0;
+#pragma unroll
+        for (int k = 0; k < 32; k++) s += ((m >> k) & 1u) ? v[k] : 0u;
+        return s;
+    } else {
+        return sum_block<BW>(blk, l, 2 * h, m & 0xFFFFu) + sum_block<BW>(blk, l, 2 * h + 1, m >> 16);
+    }
+}
+
+__device__ __forceinline__ unsigned mask32_block_rt(unsigned bw, const uint64_t *blk, unsigned l, unsigned h,
+                                                    const Pred &p, bool &bad) {
+    switch (bw) {
+#define MS_X(B) \
+    case B: return mask32_block<B>(blk, l, h, p);
+        MS_BW_CASES(MS_X)
+#undef MS_X
+    default: bad = true; return 0;
+    }
+}
+
+__device__ __forceinline__ uint64_t sum32_block_rt(unsigned bw, const uint64_t *blk, unsigned l, unsigned h,
+                                                   unsigned m, bool &bad) {
+    switch (bw) {
+#define MS_X(B) \
+    case B: return sum32_block<B>(blk, l, h, m);
+        MS_BW_CASES(MS_X)
+#undef MS_X
+    default: bad = true; return 0;
+    }
+}
+
+}  // namespace ms

@@ -62,7 +62,7 @@ ms_tuning tuning();
 
 // Staged (TMA) fused select/sum: see sps_tma.cu.
 int sps_tma(const ColView &x, const ColView &y, bool has_y, int cmp, uint64_t val, unsigned warps, unsigned stages,
-            unsigned stage_bytes, unsigned ctas_per_sm, uint64_t *d_sum, uint64_t *d_cnt, unsigned *d_err,
-            cudaStream_t st);
+            unsigned stage_bytes, unsigned ctas_per_sm, unsigned vpt, uint64_t *d_sum, uint64_t *d_cnt,
+            unsigned *d_err, cudaStream_t st);
 
 }  // namespace ms

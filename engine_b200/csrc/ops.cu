@@ -253,7 +253,8 @@ static int launch_sps(const ColView &x, const ColView &y, int cmp, uint64_t c, u
     if (!nbt) return MS_OK;
     const ms_tuning t = tuning();
     if (t.staged)
-        return sps_tma(x, y, true, cmp, c, t.warps, t.stages, t.stage_bytes, t.ctas_per_sm, d_sum, d_count, d_err, st);
+        return sps_tma(x, y, true, cmp, c, t.warps, t.stages, t.stage_bytes, t.ctas_per_sm, t.values_per_thread, d_sum,
+                       d_count, d_err, st);
     k_sps<true, true><<<grid_for_blocks(nbt), 256, 0, st>>>(x, y, cmp, c, (unsigned long long *)d_sum,
                                                             (unsigned long long *)d_count, nullptr, d_err);
     MS_CUDA_TRY(cudaGetLastError());

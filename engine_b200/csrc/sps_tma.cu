@@ -57,7 +57,7 @@ struct StageDesc {
     unsigned pad;
 };
 
-template <int W, bool kHasY, bool kFast>
+template <int W, bool kHasY, bool kFast, int VPT>
 __global__ void __launch_bounds__(32 * (W + 1), 1)
     k_sps_tma(ColView x, ColView y, StreamCol xs, StreamCol ys, int cmp, uint64_t val, Pred pred, TmaCfg cfg,
               unsigned long long *__restrict__ d_sum, unsigned long long *__restrict__ d_cnt, unsigned *err) {
@@ -172,10 +172,46 @@ __global__ void __launch_bounds__(32 * (W + 1), 1)
             const unsigned T = desc[st].nblk;
             if (T == 0) break;
             const uint64_t b0 = desc[st].b0;
+            // blocks are dealt to warps round-robin across tiles, so a tile size
+            // that is not a multiple of W does not load one warp systematically
+            const unsigned j0 = unsigned((cw + W - (b0 - b_lo) % W) % W);
+            if (kFast && VPT == 32) {
+                // two blocks per warp, one per half-warp, 32 values per thread;
+                // pairs of blocks are dealt to warps round-robin
+                bool bad = false;
+                const uint64_t base = b0 - b_lo;
+                const unsigned hb = lane >> 4, h = (lane >> 3) & 1u;
+                const uint64_t p_lo = base >> 1, p_hi = (base + T - 1) >> 1;
+                for (uint64_t P = p_lo + (cw + W - p_lo % W) % W; P <= p_hi; P += W) {
+                    const int64_t jj = int64_t(2 * P + hb) - int64_t(base);
+                    const bool act = jj >= 0 && jj < int64_t(T);
+                    const unsigned j = act ? unsigned(jj) : 0;
+                    unsigned m = 0;
+                    if (act)
+                        m = mask32_block_rt(xbw[st * kMaxTile + j],
+                                            reinterpret_cast<const uint64_t *>(ring + xoff[st * kMaxTile + j]), l, h,
+                                            pred, bad);
+                    s_cnt += __popc(m);
+                    if (act) {
+                        if (kHasY)
+                            s_sum += sum32_block_rt(ybw[st * kMaxTile + j],
+                                                    reinterpret_cast<const uint64_t *>(ring + yoff[st * kMaxTile + j]),
+                                                    l, h, m, bad);
+                        else
+                            s_sum += sum32_block_rt(xbw[st * kMaxTile + j],
+                                                    reinterpret_cast<const uint64_t *>(ring + xoff[st * kMaxTile + j]),
+                                                    l, h, m, bad);
+                    }
+                }
+                ok &= !bad;
+                __syncwarp();
+                if (lane == 0) mbar_arrive(empty + st);
+                continue;
+            }
             if (kFast) {
                 // plain vbp blocks: predicate and sum inside the bit-width switch
                 bool bad = false;
-                for (unsigned j = cw; j < T; j += W) {
+                for (unsigned j = j0; j < T; j += W) {
                     const unsigned m = mask_block_rt(
                         xbw[st * kMaxTile + j], reinterpret_cast<const uint64_t *>(ring + xoff[st * kMaxTile + j]), l,
                         q, pred, bad);
@@ -196,7 +232,7 @@ __global__ void __launch_bounds__(32 * (W + 1), 1)
                 if (lane == 0) mbar_arrive(empty + st);
                 continue;
             }
-            for (unsigned j = cw; j < T; j += W) {
+            for (unsigned j = j0; j < T; j += W) {
                 const uint64_t blk = b0 + j;
                 uint64_t v[16];
                 ok &= vbp_decode16_rt<true>(xbw[st * kMaxTile + j],
@@ -300,12 +336,12 @@ bool plain(const ColView &v) {
     return v.fmt == MS_FMT_UNCOMPR || v.fmt == MS_FMT_STATIC_VBP || v.fmt == MS_FMT_DYNAMIC_VBP;
 }
 
-template <int W, bool kHasY, bool kFast>
+template <int W, bool kHasY, bool kFast, int VPT>
 int launch_tma3(const ColView &x, const ColView &y, int cmp, uint64_t val, const TmaCfg &cfg, uint64_t *d_sum,
                 uint64_t *d_cnt, unsigned *d_err, unsigned grid, cudaStream_t st) {
     const size_t meta = align_up(16ull * cfg.stages + sizeof(StageDesc) * cfg.stages + 10ull * cfg.stages * kMaxTile, 128);
     const size_t shm = meta + size_t(cfg.stages) * cfg.stage_bytes;
-    auto kern = k_sps_tma<W, kHasY, kFast>;
+    auto kern = k_sps_tma<W, kHasY, kFast, VPT>;
     MS_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
     kern<<<grid, 32 * (W + 1), shm, st>>>(x, y, stream_of(x), stream_of(y), cmp, val, make_pred(cmp, val), cfg,
                                           (unsigned long long *)d_sum, (unsigned long long *)d_cnt, d_err);
@@ -322,11 +358,13 @@ int launch_tma3(const ColView &x, const ColView &y, int cmp, uint64_t val, const
 }
 
 template <int W, bool kHasY>
-int launch_tma(const ColView &x, const ColView &y, int cmp, uint64_t val, const TmaCfg &cfg, uint64_t *d_sum,
-               uint64_t *d_cnt, unsigned *d_err, unsigned grid, cudaStream_t st) {
-    if (plain(x) && (!kHasY || plain(y)))
-        return launch_tma3<W, kHasY, true>(x, y, cmp, val, cfg, d_sum, d_cnt, d_err, grid, st);
-    return launch_tma3<W, kHasY, false>(x, y, cmp, val, cfg, d_sum, d_cnt, d_err, grid, st);
+int launch_tma(const ColView &x, const ColView &y, int cmp, uint64_t val, const TmaCfg &cfg, unsigned vpt,
+               uint64_t *d_sum, uint64_t *d_cnt, unsigned *d_err, unsigned grid, cudaStream_t st) {
+    if (plain(x) && (!kHasY || plain(y))) {
+        if (vpt == 32) return launch_tma3<W, kHasY, true, 32>(x, y, cmp, val, cfg, d_sum, d_cnt, d_err, grid, st);
+        return launch_tma3<W, kHasY, true, 16>(x, y, cmp, val, cfg, d_sum, d_cnt, d_err, grid, st);
+    }
+    return launch_tma3<W, kHasY, false, 16>(x, y, cmp, val, cfg, d_sum, d_cnt, d_err, grid, st);
 }
 
 }  // namespace
@@ -335,16 +373,16 @@ int launch_tma(const ColView &x, const ColView &y, int cmp, uint64_t val, const 
 // must be uncompr / static_vbp or carry a block index (dynamic_vbp, for_f)
 // or a prepared delta view.  warps: consumer warps per CTA (4, 8, 12, 16, 24).
 int sps_tma(const ColView &x, const ColView &y, bool has_y, int cmp, uint64_t val, unsigned warps, unsigned stages,
-            unsigned stage_bytes, unsigned ctas_per_sm, uint64_t *d_sum, uint64_t *d_cnt, unsigned *d_err,
-            cudaStream_t st) {
+            unsigned stage_bytes, unsigned ctas_per_sm, unsigned vpt, uint64_t *d_sum, uint64_t *d_cnt,
+            unsigned *d_err, cudaStream_t st) {
     if (stage_bytes < 2 * 4096 + 128 || stage_bytes % 128) return ms_fail(MS_ERR_INVALID, "sps_tma: stage_bytes");
     if (stages < 2 || stages > 32) return ms_fail(MS_ERR_INVALID, "sps_tma: stages");
     TmaCfg cfg{stages, stage_bytes, kMaxTile};
     const unsigned grid = unsigned(sm_count()) * (ctas_per_sm ? ctas_per_sm : 1);
 #define MS_L(Wn)                                                                                          \
     if (warps == Wn)                                                                                      \
-        return has_y ? launch_tma<Wn, true>(x, y, cmp, val, cfg, d_sum, d_cnt, d_err, grid, st)           \
-                     : launch_tma<Wn, false>(x, x, cmp, val, cfg, d_sum, d_cnt, d_err, grid, st);
+        return has_y ? launch_tma<Wn, true>(x, y, cmp, val, cfg, vpt, d_sum, d_cnt, d_err, grid, st)      \
+                     : launch_tma<Wn, false>(x, x, cmp, val, cfg, vpt, d_sum, d_cnt, d_err, grid, st);
     MS_L(4) MS_L(8) MS_L(12) MS_L(16) MS_L(24)
 #undef MS_L
     return ms_fail(MS_ERR_INVALID, "sps_tma: warps must be 4, 8, 12, 16 or 24");

@@ -113,6 +113,7 @@ typedef struct ms_tuning {
     unsigned stages;
     unsigned stage_bytes;
     unsigned ctas_per_sm;
+    unsigned values_per_thread; /* 16: one warp per 512-row block; 32: two blocks per warp */
 } ms_tuning;
 int ms_gpu_set_tuning(const ms_tuning *t);
 int ms_gpu_get_tuning(ms_tuning *t);

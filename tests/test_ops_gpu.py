@@ -124,3 +124,32 @@ def test_select_project_sum(ms, arena, orc, xcode, xbw, ycode, ybw, n):
     assert (s, k) == (es, ek)
     assert np.array_equal(pos, epos)
     assert np.array_equal(vals, y[epos.astype(np.int64)])
+
+
+@pytest.mark.parametrize("cfg", [
+    dict(staged=0),
+    dict(staged=1, warps=8, stages=3, stage_bytes=16384, values_per_thread=16),
+    dict(staged=1, warps=24, stages=4, stage_bytes=49152, values_per_thread=16),
+    dict(staged=1, warps=12, stages=6, stage_bytes=24576, values_per_thread=32),
+    dict(staged=1, warps=24, stages=4, stage_bytes=49152, values_per_thread=32),
+])
+@pytest.mark.parametrize("xcode,ycode", [(O.DYNAMIC_VBP, O.DYNAMIC_VBP), (O.STATIC_VBP, O.UNCOMPR),
+                                         (O.FOR_DVBP, O.DELTA_DVBP)])
+def test_select_project_sum_every_launch_config(ms, arena, orc, cfg, xcode, ycode):
+    """Every kernel variant the autotuner can pick gives the oracle's result,
+    including odd tile/warp splits, odd bit widths and 33..64-bit blocks."""
+    n = (1 << 18) + 4321
+    x = orc.uniform_bits(77, 13, n)
+    x[::7] >>= np.uint64(6)           # blocks of mixed widths
+    y = orc.uniform_bits(78, 40, n) if ycode != O.DELTA_DVBP else orc.sorted_gaps(3, orc.geom_table(0.25), n)
+    xc = _col(ms, arena, orc, x, xcode, 13)
+    yc = _col(ms, arena, orc, y, ycode, 0)
+    old = ms.get_tuning()
+    try:
+        ms.set_tuning(**{**old, **cfg})
+        for cmp, c in ((O.CMP_LT, 900), (O.CMP_GE, 4000), (O.CMP_EQ, 17), (O.CMP_LE, 0)):
+            s, k = ms.select_project_sum(xc, cmp, c, yc)
+            sf = orc.scalar_from(xcode, 13, xc.meta())
+            assert (s, k) == orc.select_project_sum(cmp, c, x, y, sf), (cmp, c)
+    finally:
+        ms.set_tuning(**old)
