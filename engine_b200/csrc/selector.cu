@@ -72,76 +72,111 @@ __device__ __forceinline__ uint64_t wor(uint64_t x) {
     return x;
 }
 
-// One warp per block.  Thread `lane` reads rows j = k*32 + lane (k = 0..63):
-// row j belongs to sub-block k/16 and TVL lane j%8 = lane%8.
+// Analysis of one block by one warp.  Thread `lane` reads rows
+// j = k*32 + lane (k = 0..63): row j belongs to sub-block k/16 and TVL lane
+// j%8 = lane%8.
+__device__ BlockStats analyze_block(const uint64_t *__restrict__ x, unsigned lane) {
+    BlockStats s;
+    uint64_t prev = 0;       // x[j - 32] of this thread (previous k)
+    uint64_t last_prev = 0;  // x[j - 1] for lane 0: lane 31 of the previous k
+    unsigned heads = 0;
+    int64_t mn[2] = {INT64_MAX, INT64_MAX};
+#pragma unroll 4
+    for (unsigned i = 0; i < 4; i++) {
+        uint64_t o_raw = 1, o_dlt = 1;
+#pragma unroll
+        for (unsigned kk = 0; kk < 16; kk++) {
+            const unsigned k = i * 16 + kk;
+            const uint64_t v = __ldg(x + k * 32 + lane);
+            // x[j-8]: lane-8 of this k, or lane+24 of the previous k
+            const uint64_t up8 = __shfl_up_sync(0xFFFFFFFFu, v, 8);
+            const uint64_t pk = __shfl_sync(0xFFFFFFFFu, prev, (lane + 24) & 31u);
+            const uint64_t x8 = lane >= 8 ? up8 : (k ? pk : 0);
+            const uint64_t up1 = __shfl_up_sync(0xFFFFFFFFu, v, 1);
+            const uint64_t x1 = lane >= 1 ? up1 : last_prev;
+            heads += (k == 0 && lane == 0) ? 1u : unsigned(v != x1);
+            o_raw |= v;
+            o_dlt |= v - x8;
+            mn[i >> 1] = min(mn[i >> 1], (int64_t)v);
+            last_prev = __shfl_sync(0xFFFFFFFFu, v, 31);
+            prev = v;
+        }
+        s.raw[i] = uint8_t(effective_bitwidth(wor(o_raw)));
+        s.dlt[i] = uint8_t(effective_bitwidth(wor(o_dlt)));
+    }
+    // FOR references: signed minimum per TVL lane, unsigned across lanes
+    for (unsigned hh = 0; hh < 2; hh++) {
+        int64_t m = mn[hh];
+        m = min(m, (int64_t)__shfl_xor_sync(0xFFFFFFFFu, (uint64_t)m, 8));
+        m = min(m, (int64_t)__shfl_xor_sync(0xFFFFFFFFu, (uint64_t)m, 16));
+        uint64_t um = (uint64_t)m;
+        um = minu(um, __shfl_xor_sync(0xFFFFFFFFu, um, 1));
+        um = minu(um, __shfl_xor_sync(0xFFFFFFFFu, um, 2));
+        um = minu(um, __shfl_xor_sync(0xFFFFFFFFu, um, 4));
+        if (um == ~uint64_t(0)) um--;
+        s.ref[hh] = um;
+    }
+    // FOR offsets (second read of the block, from L1/L2)
+#pragma unroll 4
+    for (unsigned i = 0; i < 4; i++) {
+        uint64_t o = 1;
+        const uint64_t ref = s.ref[i >> 1];
+#pragma unroll
+        for (unsigned kk = 0; kk < 16; kk++) o |= __ldg(x + (i * 16 + kk) * 32 + lane) - ref;
+        s.fr[i] = uint8_t(effective_bitwidth(wor(o)));
+    }
+    s.runs = __reduce_add_sync(0xFFFFFFFFu, heads);
+    s.sbw = uint8_t(max(max(s.raw[0], s.raw[1]), max(s.raw[2], s.raw[3])));
+    s.pad[0] = s.pad[1] = s.pad[2] = 0;
+    return s;
+}
+
+__device__ __forceinline__ unsigned best_cand(const BlockStats &s) {
+    unsigned best = 0;
+    uint32_t bs = cand_size(s, 0);
+    for (unsigned c = 1; c < kSelNC; c++)
+        if (cand_size(s, c) < bs) {
+            bs = cand_size(s, c);
+            best = c;
+        }
+    return best;
+}
+
 __global__ void __launch_bounds__(256) k_sel_analyze(const uint64_t *__restrict__ in, uint64_t nblk,
                                                     BlockStats *__restrict__ st, uint32_t *__restrict__ sizes) {
     const unsigned lane = threadIdx.x & 31u;
     for (uint64_t b = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) / 32; b < nblk;
          b += uint64_t(gridDim.x) * blockDim.x / 32) {
-        const uint64_t *x = in + b * kSelBlock;
-        BlockStats s;
-        uint64_t prev = 0;      // x[j - 32] of this thread (previous k)
-        uint64_t last_prev = 0; // x[j - 1] for lane 0: lane 31 of the previous k
-        unsigned heads = 0;
-        int64_t mn[2] = {INT64_MAX, INT64_MAX};
-#pragma unroll 4
-        for (unsigned i = 0; i < 4; i++) {
-            uint64_t o_raw = 1, o_dlt = 1;
-#pragma unroll
-            for (unsigned kk = 0; kk < 16; kk++) {
-                const unsigned k = i * 16 + kk;
-                const uint64_t v = __ldg(x + k * 32 + lane);
-                // x[j-8]: lane-8 of this k, or lane+24 of the previous k
-                const uint64_t up8 = __shfl_up_sync(0xFFFFFFFFu, v, 8);
-                const uint64_t pk = __shfl_sync(0xFFFFFFFFu, prev, (lane + 24) & 31u);
-                const uint64_t x8 = lane >= 8 ? up8 : (k ? pk : 0);
-                const uint64_t up1 = __shfl_up_sync(0xFFFFFFFFu, v, 1);
-                const uint64_t x1 = lane >= 1 ? up1 : last_prev;
-                heads += (k == 0 && lane == 0) ? 1u : unsigned(v != x1);
-                o_raw |= v;
-                o_dlt |= v - x8;
-                mn[i >> 1] = min(mn[i >> 1], (int64_t)v);
-                last_prev = __shfl_sync(0xFFFFFFFFu, v, 31);
-                prev = v;
-            }
-            o_raw = wor(o_raw);
-            o_dlt = wor(o_dlt);
-            s.raw[i] = uint8_t(effective_bitwidth(o_raw));
-            s.dlt[i] = uint8_t(effective_bitwidth(o_dlt));
-        }
-        // FOR references: signed minimum per TVL lane, unsigned across lanes
-        for (unsigned hh = 0; hh < 2; hh++) {
-            int64_t m = mn[hh];
-            m = min(m, (int64_t)__shfl_xor_sync(0xFFFFFFFFu, (uint64_t)m, 8));
-            m = min(m, (int64_t)__shfl_xor_sync(0xFFFFFFFFu, (uint64_t)m, 16));
-            uint64_t um = (uint64_t)m;
-            um = minu(um, __shfl_xor_sync(0xFFFFFFFFu, um, 1));
-            um = minu(um, __shfl_xor_sync(0xFFFFFFFFu, um, 2));
-            um = minu(um, __shfl_xor_sync(0xFFFFFFFFu, um, 4));
-            if (um == ~uint64_t(0)) um--;
-            s.ref[hh] = um;
-        }
-        // FOR offsets (second read of the block, from L1/L2)
-#pragma unroll 4
-        for (unsigned i = 0; i < 4; i++) {
-            uint64_t o = 1;
-            const uint64_t ref = s.ref[i >> 1];
-#pragma unroll
-            for (unsigned kk = 0; kk < 16; kk++) o |= __ldg(x + (i * 16 + kk) * 32 + lane) - ref;
-            s.fr[i] = uint8_t(effective_bitwidth(wor(o)));
-        }
-        heads = __reduce_add_sync(0xFFFFFFFFu, heads);
-        s.runs = heads;
-        const unsigned mx = max(max(s.raw[0], s.raw[1]), max(s.raw[2], s.raw[3]));
-        s.sbw = uint8_t(mx);
-        s.pad[0] = s.pad[1] = s.pad[2] = 0;
+        const BlockStats s = analyze_block(in + b * kSelBlock, lane);
         if (lane == 0) {
             st[b] = s;
             if (sizes)
                 for (unsigned c = 0; c < kSelNC; c++) sizes[b * kSelNC + c] = cand_size(s, c);
         }
     }
+}
+
+// Exhaustive decision for the blocks the learned selector left open
+// (choice 255); the others keep their choice.
+__global__ void __launch_bounds__(256) k_sel_resolve(const uint64_t *__restrict__ in, uint64_t nblk,
+                                                    uint8_t *__restrict__ choice) {
+    const unsigned lane = threadIdx.x & 31u;
+    for (uint64_t b = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) / 32; b < nblk;
+         b += uint64_t(gridDim.x) * blockDim.x / 32) {
+        if (choice[b] != 255) continue;
+        const BlockStats s = analyze_block(in + b * kSelBlock, lane);
+        if (lane == 0) choice[b] = uint8_t(best_cand(s));
+    }
+}
+
+// Footprint of a choice vector given exact sizes.
+__global__ void k_sel_footprint(const uint32_t *__restrict__ sizes, const uint8_t *__restrict__ choice, uint64_t nblk,
+                                unsigned long long *__restrict__ total) {
+    uint64_t t = 0;
+    for (uint64_t b = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; b < nblk; b += uint64_t(gridDim.x) * blockDim.x)
+        t += sizes[b * kSelNC + (choice[b] < kSelNC ? choice[b] : 0)];
+    for (int s = 16; s > 0; s >>= 1) t += __shfl_xor_sync(0xFFFFFFFFu, t, s);
+    if ((threadIdx.x & 31u) == 0) atomicAdd(total, (unsigned long long)t);
 }
 
 // Write block b (values x) in candidate c at out (64-B aligned).  The warp's
@@ -516,5 +551,236 @@ extern "C" int ms_gpu_bwi_compress(const uint64_t *d_in, uint64_t nblk, const vo
     *d_out = out;
     *d_offsets = off;
     *h_bytes = bytes;
+    return MS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Mixed synthetic column for the selector: segments of `seg_blocks` blocks
+// cycle through four families (by segment index and seed): uniform over b
+// bits (b in 1..40), sorted with random gaps, long runs, Zipf (inverse-CDF
+// table).  One warp per block; value j of the block is row k*32 + lane.
+// ---------------------------------------------------------------------------
+namespace ms {
+namespace {
+
+__device__ __forceinline__ uint64_t gmix(uint64_t seed, uint64_t i) {
+    uint64_t z = seed + (i + 1) * 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+__global__ void __launch_bounds__(256) k_sel_gen(uint64_t seed, uint64_t nblk, unsigned seg_blocks,
+                                                const uint64_t *__restrict__ zipf, uint64_t n_zipf,
+                                                uint64_t *__restrict__ out) {
+    const unsigned lane = threadIdx.x & 31u;
+    for (uint64_t b = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) / 32; b < nblk;
+         b += uint64_t(gridDim.x) * blockDim.x / 32) {
+        const uint64_t seg = b / seg_blocks;
+        const uint64_t h = gmix(seed, seg);
+        const unsigned fam = unsigned((seg + seed) & 3u);
+        uint64_t *o = out + b * kSelBlock;
+        const uint64_t rs = gmix(seed ^ 0xA5A5A5A5ull, b);
+        if (fam == 0) {  // uniform over b bits
+            const unsigned bits = 1 + unsigned(h % 40);
+            for (unsigned k = 0; k < 64; k++) o[k * 32 + lane] = gmix(rs, k * 32 + lane) >> (64 - bits);
+        } else if (fam == 3) {  // Zipf over the table's range
+            for (unsigned k = 0; k < 64; k++) {
+                const uint64_t u = gmix(rs, k * 32 + lane);
+                uint64_t lo = 0, hi = n_zipf - 1;
+                while (lo < hi) {
+                    const uint64_t mid = (lo + hi) >> 1;
+                    if (u < zipf[mid]) hi = mid;
+                    else lo = mid + 1;
+                }
+                o[k * 32 + lane] = lo;
+            }
+        } else {
+            // sorted: prefix sums of gaps in [1, 2g-1]; runs: value changes
+            // where a draw hits 1/L, run values over 20 bits
+            const unsigned g = 1 + unsigned(h % 16);
+            const unsigned L = 64u << unsigned((h >> 8) % 4);
+            uint64_t carry = fam == 1 ? (rs >> 24) : 0;
+            for (unsigned k = 0; k < 64; k++) {
+                const uint64_t u = gmix(rs, k * 32 + lane);
+                uint64_t inc = fam == 1 ? 1 + u % (2 * g - 1) : uint64_t(u % L == 0);
+                // inclusive warp scan
+#pragma unroll
+                for (int s = 1; s < 32; s <<= 1) {
+                    const uint64_t t = __shfl_up_sync(0xFFFFFFFFu, inc, s);
+                    if (lane >= unsigned(s)) inc += t;
+                }
+                const uint64_t v = carry + inc;
+                o[k * 32 + lane] = fam == 1 ? v : (gmix(rs ^ 0x77, v) >> 44);
+                carry = __shfl_sync(0xFFFFFFFFu, v, 31);
+            }
+        }
+    }
+}
+
+// select(value cmp c) -> sum over a blockwise container.  One warp per
+// block; the four 512-row sub-blocks are decoded with the vbp decoder, the
+// cascade steps applied per format, rle handled per run.
+__global__ void __launch_bounds__(256) k_bwi_select_sum(const uint8_t *__restrict__ data,
+                                                       const uint64_t *__restrict__ q, const uint8_t *__restrict__ codes,
+                                                       const uint32_t *__restrict__ psz, uint64_t nblk, int cmp,
+                                                       uint64_t val,
+                                                       unsigned long long *__restrict__ d_sum,
+                                                       unsigned long long *__restrict__ d_cnt, unsigned *err) {
+    const unsigned lane = threadIdx.x & 31u, l = lane & 7u, qq = lane >> 3;
+    uint64_t s_sum = 0, s_cnt = 0;
+    bool ok = true;
+    for (uint64_t b = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) / 32; b < nblk;
+         b += uint64_t(gridDim.x) * blockDim.x / 32) {
+        const unsigned code = codes[b];
+        const uint8_t *p = data + q[b] + 64;
+        if (code == 71) {  // rle: (value, length) pairs covering 2048 rows
+            const uint64_t *pr = reinterpret_cast<const uint64_t *>(p);
+            const unsigned runs = psz[b] / 16;
+            uint64_t rows = 0;
+            for (unsigned r0 = 0; r0 < runs; r0 += 32) {
+                const unsigned r = r0 + lane;
+                if (r < runs) {
+                    const uint64_t v = pr[2 * r], len = pr[2 * r + 1];
+                    rows += len;
+                    if (cmp_eval(cmp, v, val, true)) {
+                        s_sum += v * len;
+                        s_cnt += len;
+                    }
+                }
+            }
+            ok &= __reduce_add_sync(0xFFFFFFFFu, unsigned(rows)) == kSelBlock;
+            continue;
+        }
+        // per sub-block location and width
+        uint64_t carry = 0;  // delta: running lane sum
+        for (unsigned i = 0; i < 4; i++) {
+            unsigned bw;
+            uint64_t off, ref = 0;
+            bool dlt = false;
+            if (code >= 1 && code <= 64) {
+                bw = code;
+                off = uint64_t(64) * bw * i;
+            } else if (code == 65) {
+                uint64_t acc = 0;
+                for (unsigned k = 0; k < i; k++) acc += p[k];
+                bw = p[i];
+                off = 64 + 64 * acc;
+            } else if (code == 67 || code == 69) {
+                const bool isfor = code == 69;
+                const uint64_t page0 = isfor ? 64 : 0;
+                const uint8_t w0 = p[page0], w1 = p[page0 + 1];
+                const uint64_t page1 = page0 + 64 + 64 * uint64_t(w0 + w1);
+                const uint64_t pg = (i >> 1) ? page1 : page0;
+                const uint8_t a = p[pg], c2 = p[pg + 1];
+                bw = (i & 1) ? c2 : a;
+                off = pg + 64 + ((i & 1) ? 64 * uint64_t(a) : 0);
+                if (isfor) ref = reinterpret_cast<const uint64_t *>(p)[i >> 1];
+                else dlt = true;
+            } else {
+                ok = false;
+                break;
+            }
+            uint64_t v[16];
+            ok &= vbp_decode16_rt(bw, reinterpret_cast<const uint64_t *>(p + off), l, qq, v);
+            if (dlt) {
+#pragma unroll
+                for (int k = 1; k < 16; k++) v[k] += v[k - 1];
+                const uint64_t tot = v[15];
+                const uint64_t up = __shfl_up_sync(0xFFFFFFFFu, tot, 8);
+                uint64_t pre = qq >= 1 ? up : 0;
+                const uint64_t up2 = __shfl_up_sync(0xFFFFFFFFu, tot + pre, 16);
+                pre += qq >= 2 ? up2 : 0;
+                pre += carry;
+#pragma unroll
+                for (int k = 0; k < 16; k++) v[k] += pre;
+                // lane total of this sub-block: last value of quarter 3
+                carry = __shfl_sync(0xFFFFFFFFu, v[15], 24 + l);
+            } else {
+#pragma unroll
+                for (int k = 0; k < 16; k++) v[k] += ref;
+            }
+#pragma unroll
+            for (int k = 0; k < 16; k++)
+                if (cmp_eval(cmp, v[k], val, true)) {
+                    s_sum += v[k];
+                    s_cnt++;
+                }
+        }
+    }
+    if (!ok) atomicOr(err, kErrCorrupt);
+    for (int s = 16; s > 0; s >>= 1) {
+        s_sum += __shfl_xor_sync(0xFFFFFFFFu, s_sum, s);
+        s_cnt += __shfl_xor_sync(0xFFFFFFFFu, s_cnt, s);
+    }
+    if (lane == 0) {
+        atomicAdd(d_sum, (unsigned long long)s_sum);
+        if (d_cnt) atomicAdd(d_cnt, (unsigned long long)s_cnt);
+    }
+}
+
+__global__ void k_bwi_codes(const BlockStats *__restrict__ st, const uint8_t *__restrict__ choice, uint64_t nblk,
+                            uint8_t *__restrict__ codes, uint32_t *__restrict__ psz) {
+    for (uint64_t b = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; b < nblk; b += uint64_t(gridDim.x) * blockDim.x) {
+        codes[b] = cand_code(st[b], choice[b]);
+        psz[b] = cand_size(st[b], choice[b]);
+    }
+}
+
+}  // namespace
+}  // namespace ms
+
+extern "C" int ms_gpu_sel_gen(uint64_t seed, uint64_t nblk, unsigned seg_blocks, const uint64_t *d_zipf,
+                              uint64_t n_zipf, uint64_t *d_out, void *stream) {
+    if ((!d_out || !d_zipf || !n_zipf || !seg_blocks) && nblk) return ms_fail(MS_ERR_INVALID, "sel_gen: bad argument");
+    if (!nblk) return MS_OK;
+    k_sel_gen<<<sel_grid(nblk), 256, 0, (cudaStream_t)stream>>>(seed, nblk, seg_blocks, d_zipf, n_zipf, d_out);
+    MS_CUDA_TRY(cudaGetLastError());
+    return MS_OK;
+}
+
+extern "C" int ms_gpu_sel_resolve(const uint64_t *d_in, uint64_t nblk, uint8_t *d_choice, void *stream) {
+    if ((!d_in || !d_choice) && nblk) return ms_fail(MS_ERR_INVALID, "sel_resolve: bad argument");
+    if (!nblk) return MS_OK;
+    k_sel_resolve<<<sel_grid(nblk), 256, 0, (cudaStream_t)stream>>>(d_in, nblk, d_choice);
+    MS_CUDA_TRY(cudaGetLastError());
+    return MS_OK;
+}
+
+extern "C" int ms_gpu_sel_footprint(const uint32_t *d_sizes, const uint8_t *d_choice, uint64_t nblk, uint64_t *d_total,
+                                    void *stream) {
+    if (!d_total || ((!d_sizes || !d_choice) && nblk)) return ms_fail(MS_ERR_INVALID, "sel_footprint: bad argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    MS_CUDA_TRY(cudaMemsetAsync(d_total, 0, 8, st));
+    if (!nblk) return MS_OK;
+    k_sel_footprint<<<sel_grid(nblk), 256, 0, st>>>(d_sizes, d_choice, nblk, (unsigned long long *)d_total);
+    MS_CUDA_TRY(cudaGetLastError());
+    return MS_OK;
+}
+
+// Block index of a container: format code and payload bytes per block.
+extern "C" int ms_gpu_bwi_codes(const void *d_stats, const uint8_t *d_choice, uint64_t nblk, uint8_t *d_codes,
+                                uint32_t *d_payload_bytes, void *stream) {
+    if ((!d_stats || !d_choice || !d_codes || !d_payload_bytes) && nblk)
+        return ms_fail(MS_ERR_INVALID, "bwi_codes: bad argument");
+    if (!nblk) return MS_OK;
+    k_bwi_codes<<<sel_grid(nblk), 256, 0, (cudaStream_t)stream>>>((const BlockStats *)d_stats, d_choice, nblk, d_codes,
+                                                                  d_payload_bytes);
+    MS_CUDA_TRY(cudaGetLastError());
+    return MS_OK;
+}
+
+extern "C" int ms_gpu_bwi_select_sum(const uint8_t *d_data, const uint64_t *d_offsets, const uint8_t *d_codes,
+                                     const uint32_t *d_payload_bytes, uint64_t nblk, int cmp, uint64_t val,
+                                     uint64_t *d_sum, uint64_t *d_cnt, unsigned *d_err, void *stream) {
+    if (!d_sum || !d_err || ((!d_data || !d_offsets || !d_codes || !d_payload_bytes) && nblk))
+        return ms_fail(MS_ERR_INVALID, "bwi_select_sum: bad argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    MS_CUDA_TRY(cudaMemsetAsync(d_sum, 0, 8, st));
+    if (d_cnt) MS_CUDA_TRY(cudaMemsetAsync(d_cnt, 0, 8, st));
+    if (!nblk) return MS_OK;
+    k_bwi_select_sum<<<sel_grid(nblk), 256, 0, st>>>(d_data, d_offsets, d_codes, d_payload_bytes, nblk, cmp, val,
+                                                    (unsigned long long *)d_sum, (unsigned long long *)d_cnt, d_err);
+    MS_CUDA_TRY(cudaGetLastError());
     return MS_OK;
 }

@@ -214,6 +214,54 @@ int ms_gpu_select_noalloc(int cmp, uint64_t val, const ms_col *in, uint64_t *d_o
                           uint64_t out_capacity, uint64_t *d_out_count, unsigned *d_err, void *stream);
 uint64_t ms_gpu_select_noalloc_max_rows(void);
 
+/* ---- per-block format selection and the learned selector ------------------
+ * Blocks of ms_gpu_sel_block_values() = 2048 values; five candidates per block
+ * (0 static_vbp<max width>, 1 dynamic_vbp, 2 delta+dvbp, 3 for+dvbp, 4 rle),
+ * each sized exactly as the reference's morph_batch of 2048 values writes it.
+ * The exhaustive judge restates exhaustive_size_format_selector.h:36-141 over
+ * these candidates; the container follows blockwise_individual_f
+ * (blockwise_individual.h:89-99): a format-code byte (format_selector_commons.h:
+ * 25-103; 71 = rle, which the reference's container lacks), padding to 64 B,
+ * the payload.  The learned selector (no counterpart in the reference) is an
+ * MLP 32 -> 64 -> 64 -> 5 over sampled block statistics predicting log2 of
+ * every candidate's size; BF16 weights, FP32 accumulation. */
+uint64_t ms_gpu_sel_block_values(void);
+uint64_t ms_gpu_sel_stats_bytes(void);
+int ms_gpu_sel_gen(uint64_t seed, uint64_t nblk, unsigned seg_blocks, const uint64_t *d_zipf_table,
+                   uint64_t n_zipf, uint64_t *d_out, void *stream);
+int ms_gpu_sel_analyze(const uint64_t *d_in, uint64_t nblk, void *d_stats, uint32_t *d_sizes, void *stream);
+uint64_t ms_gpu_sel_compress_all_scratch_bytes(void);
+int ms_gpu_sel_compress_all(const uint64_t *d_in, uint64_t nblk, void *d_stats, uint32_t *d_sizes,
+                            uint8_t *d_scratch, unsigned *d_err, void *stream);
+int ms_gpu_sel_features(const uint64_t *d_in, uint64_t nblk, float *d_feats, void *stream);
+int ms_gpu_sel_argmin(const uint32_t *d_sizes, uint64_t nblk, uint8_t *d_choice, uint64_t *d_total, void *stream);
+int ms_gpu_sel_resolve(const uint64_t *d_in, uint64_t nblk, uint8_t *d_choice, void *stream);
+int ms_gpu_sel_footprint(const uint32_t *d_sizes, const uint8_t *d_choice, uint64_t nblk, uint64_t *d_total,
+                         void *stream);
+int ms_gpu_bwi_compress(const uint64_t *d_in, uint64_t nblk, const void *d_stats, const uint8_t *d_choice,
+                        uint8_t **d_out, uint64_t **d_offsets, uint64_t *h_bytes, ms_arena *arena, void *stream);
+int ms_gpu_bwi_codes(const void *d_stats, const uint8_t *d_choice, uint64_t nblk, uint8_t *d_codes,
+                     uint32_t *d_payload_bytes, void *stream);
+int ms_gpu_bwi_select_sum(const uint8_t *d_data, const uint64_t *d_offsets, const uint8_t *d_codes,
+                          const uint32_t *d_payload_bytes, uint64_t nblk, int cmp, uint64_t val,
+                          uint64_t *d_sum, uint64_t *d_cnt, unsigned *d_err, void *stream);
+
+typedef struct ms_mlp ms_mlp;
+uint64_t ms_gpu_mlp_param_count(void);
+int ms_gpu_mlp_create(uint64_t seed, unsigned max_batch, ms_mlp **out);
+int ms_gpu_mlp_destroy(ms_mlp *m);
+int ms_gpu_mlp_train(ms_mlp *m, const float *d_feats, const uint32_t *d_sizes, uint64_t n, unsigned steps,
+                     unsigned batch, float lr, uint64_t seed, float *d_loss_curve, void *stream);
+int ms_gpu_mlp_grads(ms_mlp *m, const float *d_feats, const uint32_t *d_sizes, uint64_t n,
+                     const uint32_t *d_idx, unsigned batch, float *d_grads, float *d_loss, void *stream);
+int ms_gpu_mlp_eval_loss(ms_mlp *m, const float *d_feats, const uint32_t *d_sizes, uint64_t n,
+                         const uint32_t *d_idx, unsigned batch, float *d_loss, void *stream);
+int ms_gpu_mlp_choose(ms_mlp *m, const float *d_feats, uint64_t n, float margin_log2, float *d_pred,
+                      uint8_t *d_choice, uint64_t *d_nfallback, void *stream);
+uint64_t ms_gpu_mlp_state_bytes(void);
+int ms_gpu_mlp_save(ms_mlp *m, void *h_state);
+int ms_gpu_mlp_load(ms_mlp *m, const void *h_state);
+
 /* ---- synthetic data (device-side, counter-based splitmix64) -------------- */
 int ms_gpu_gen_uniform_bits(uint64_t seed, unsigned bits, uint64_t n, uint64_t *d_out, void *stream);
 int ms_gpu_gen_from_table(uint64_t seed, const uint64_t *d_table, uint64_t n_table, uint64_t n,
