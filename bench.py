@@ -308,6 +308,9 @@ def run_gpu(args):
             "clocks": clk.summary(), "e2e": e2e, "gpu_launches": args.steps}
     if args.log2_rows != 28:
         line["config"]["note"] = "reduced size: profiling run, not the benchmark workload"
+    if not args.no_selector and world == 1:
+        arena.close()
+        line["learned_selector"] = selector_run(ms, args)
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
             line["cpu_baseline"] = cpu_baseline(1)
@@ -318,8 +321,148 @@ def run_gpu(args):
         torch.distributed.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
-    arena.close()
+    if args.no_selector or world > 1:
+        arena.close()
     return 0 if ok else 1
+
+
+def selector_run(ms, args):
+    """Learned vs exhaustive format pick on a 2^30-value column of 64K-value
+    segments cycling through uniform-b-bit, sorted-with-gaps, long-run and
+    Zipf data; MLP trained on 2^20 labelled 2048-value blocks (2000 Adam
+    steps, batch 4096).  Times are device times (CUDA events) on this GPU."""
+    import torch
+    import oracle
+    import engine_b200.selector as S
+    orc = oracle.Oracle()
+    zipf = orc.zipf_table(1.2, 1 << 20)
+    stream = torch.cuda.current_stream()
+    arena = ms.Arena(20 << 30)
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+
+    def timed(fn, reps=3):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = ev(), ev()
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    try:
+        # --- training set: 2^20 blocks, labelled by the codecs themselves -------
+        n_train = 1 << (args.sel_log2_train)
+        chunk = 1 << 17
+        feats = arena.alloc(4 * 32 * n_train)
+        sizes = arena.alloc(4 * 5 * n_train)
+        mark = arena.used()
+        t_label = 0.0
+        for c0 in range(0, n_train, chunk):
+            nb = min(chunk, n_train - c0)
+            d = S.gen(arena, 1000 + c0, nb, 32, zipf)
+            st = arena.alloc(S.STATS_BYTES * nb)
+            e0, e1 = ev(), ev()
+            e0.record(stream)
+            ms._check(S._L.ms_gpu_sel_analyze(d, nb, st, sizes + 4 * 5 * c0, stream.cuda_stream), "analyze")
+            ms._check(S._L.ms_gpu_sel_features(d, nb, feats + 4 * 32 * c0, stream.cuda_stream), "features")
+            e1.record(stream)
+            torch.cuda.synchronize()
+            t_label += e0.elapsed_time(e1)
+            ms._check(ms.lib().ms_gpu_arena_reset(arena.h), "reset")
+            arena.alloc(mark)  # keep feats/sizes
+        m = S.Mlp(seed=1, max_batch=4096)
+        e0, e1 = ev(), ev()
+        e0.record(stream)
+        curve = m.train(arena, feats, sizes, n_train, steps=args.sel_steps, batch=4096, lr=2e-3)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t_train = e0.elapsed_time(e1)
+        # --- evaluation column: 2^30 values ------------------------------------
+        n_eval = 1 << (args.sel_log2_eval - 11)
+        col = S.gen(arena, 77, n_eval, 32, zipf)
+        scratch = arena.alloc(int(S._L.ms_gpu_sel_compress_all_scratch_bytes()))
+        st_all = arena.alloc(S.STATS_BYTES * n_eval)
+        sz_all = arena.alloc(4 * 5 * n_eval)
+        err = arena.alloc(8)
+        ch_ex = arena.alloc(n_eval)
+        tot = arena.alloc(8)
+        feats_e = arena.alloc(4 * 32 * n_eval)
+        ch_ml = arena.alloc(n_eval)
+        nfb = arena.alloc(8)
+        margin = float(np.log2(1.02))
+        sp = stream.cuda_stream
+
+        def exhaustive_materialising():
+            ms._check(S._L.ms_gpu_sel_compress_all(col, n_eval, st_all, sz_all, scratch, err, sp), "compress_all")
+            ms._check(S._L.ms_gpu_sel_argmin(sz_all, n_eval, ch_ex, tot, sp), "argmin")
+
+        def exhaustive_size_only():
+            ms._check(S._L.ms_gpu_sel_analyze(col, n_eval, st_all, sz_all, sp), "analyze")
+            ms._check(S._L.ms_gpu_sel_argmin(sz_all, n_eval, ch_ex, tot, sp), "argmin")
+
+        def learned():
+            ms._check(S._L.ms_gpu_sel_features(col, n_eval, feats_e, sp), "features")
+            ms._check(S._L.ms_gpu_mlp_choose(m.h, feats_e, n_eval, margin, None, ch_ml, nfb, sp), "choose")
+            ms._check(S._L.ms_gpu_sel_resolve(col, n_eval, ch_ml, sp), "resolve")
+
+        t_all = timed(exhaustive_materialising)
+        t_size = timed(exhaustive_size_only)
+        t_ml = timed(learned)
+        exhaustive_size_only()
+        n_fb = int(S.to_host(nfb, 1, np.uint64)[0])
+        fp_ex = S.footprint(arena, sz_all, ch_ex, n_eval)
+        fp_ml = S.footprint(arena, sz_all, ch_ml, n_eval)
+        picks = np.bincount(S.to_host(ch_ml, n_eval, np.uint8), minlength=5).tolist()
+        # --- end to end: selection + compression + select-sum ------------------
+        cmp_val = 1 << 20
+        tv = ms._device_view(col, 8 * n_eval * S.BLOCK).view(torch.int64)
+        hit = tv < cmp_val  # values stay below 2^63: signed compare as the operator's
+        exp_s = int(torch.where(hit, tv, torch.zeros_like(tv)).sum().item()) & ((1 << 64) - 1)
+        exp_c = int(hit.sum().item())
+        del tv, hit
+        results = {}
+        for name, pick in (("exhaustive", ch_ex), ("learned", ch_ml)):
+            mark2 = arena.used()
+
+            def e2e(pick=pick, name=name):
+                ms._check(ms.lib().ms_gpu_arena_reset(arena.h), "reset")
+                arena.alloc(mark2)
+                if name == "exhaustive":
+                    exhaustive_materialising()
+                    stp = st_all
+                else:
+                    learned()
+                    ms._check(S._L.ms_gpu_sel_analyze(col, n_eval, st_all, None, sp), "analyze")
+                    stp = st_all
+                cont = S.Container(arena, col, n_eval, stp, pick, stream=stream)
+                results[name] = cont.select_sum(oracle.CMP_LT, cmp_val, stream=stream) + (cont.nbytes,)
+
+            results[name + "_ms"] = timed(e2e, reps=2)
+        ok = (results["exhaustive"][:2] == (exp_s, exp_c) and results["learned"][:2] == (exp_s, exp_c)
+              and results["exhaustive"][2] == 0 and results["learned"][2] == 0)
+        m.close()
+        return {
+            "workload": "2^%d-value column, 64K-value segments cycling uniform(1..40 bit)/sorted/runs/Zipf(1.2); "
+                        "2048-value blocks; candidates static_vbp, dynamic_vbp, delta+dvbp, for+dvbp, rle"
+                        % args.sel_log2_eval,
+            "train": {"blocks": n_train, "steps": args.sel_steps, "batch": 4096, "ms": round(t_train, 1),
+                      "label_and_feature_ms": round(t_label, 1), "loss_first": float(curve[:10].mean()),
+                      "loss_last": float(curve[-10:].mean())},
+            "footprint_bytes": {"exhaustive": fp_ex, "learned": fp_ml},
+            "regret": round(fp_ml / fp_ex - 1, 5),
+            "fallback_fraction": round(n_fb / n_eval, 4),
+            "picks": dict(zip(S.CAND_NAMES, picks)),
+            "selection_ms": {"compress_all": round(t_all, 3), "exhaustive_size_only": round(t_size, 3),
+                             "learned": round(t_ml, 3)},
+            "selection_speedup_vs_compress_all": round(t_all / t_ml, 2),
+            "e2e_ms": {"exhaustive": round(results["exhaustive_ms"], 3), "learned": round(results["learned_ms"], 3)},
+            "container_bytes": {"exhaustive": results["exhaustive"][3], "learned": results["learned"][3]},
+            "select_sum_bit_exact": ok,
+        }
+    finally:
+        arena.close()
 
 
 def e2e_run(ms, lib, arena, xc, yc, sp, args, exp_sum):
@@ -385,6 +528,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffer) leg")
     ap.add_argument("--log2-rows", type=int, default=28, help="rows per GPU = 2^N (profiling runs use less)")
+    ap.add_argument("--no-selector", action="store_true", help="skip the learned-vs-exhaustive selector leg")
+    ap.add_argument("--sel-log2-train", type=int, default=20, help="training blocks = 2^N")
+    ap.add_argument("--sel-log2-eval", type=int, default=30, help="evaluation column values = 2^N")
+    ap.add_argument("--sel-steps", type=int, default=2000, help="Adam steps")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -266,6 +266,13 @@ int ms_gpu_mlp_load(ms_mlp *m, const void *h_state);
 int ms_gpu_gen_uniform_bits(uint64_t seed, unsigned bits, uint64_t n, uint64_t *d_out, void *stream);
 int ms_gpu_gen_from_table(uint64_t seed, const uint64_t *d_table, uint64_t n_table, uint64_t n,
                           uint64_t *d_out, void *stream);
+/* sorted ascending: prefix sums of 1 + (draw from the gap table) */
+int ms_gpu_gen_sorted_gaps(uint64_t seed, const uint64_t *d_gap_table, uint64_t n_table, uint64_t n,
+                           uint64_t *d_out, ms_arena *arena, void *stream);
+/* runs: a new run at row i > 0 with probability 2^-log2_mean_len, run values
+ * over value_bits bits */
+int ms_gpu_gen_runs(uint64_t seed, unsigned log2_mean_len, unsigned value_bits, uint64_t n, uint64_t *d_out,
+                    ms_arena *arena, void *stream);
 
 #ifdef __cplusplus
 }
