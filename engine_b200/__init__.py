@@ -82,6 +82,8 @@ _sig = {
     "ms_gpu_intersect_sorted": (C.c_int, [_P(MsCol), _P(MsCol), C.c_int, C.c_uint, _P(MsCol), _V, _V]),
     "ms_gpu_group": (C.c_int, [_P(MsCol), _P(MsCol), C.c_int, _P(MsCol), C.c_int, _P(MsCol), _V, _V]),
     "ms_gpu_agg_sum_grouped": (C.c_int, [_P(MsCol), _P(MsCol), _U64, _P(MsCol), _V, _V]),
+    "ms_gpu_query3": (C.c_int, [_P(MsCol), C.c_int, _U64, _P(MsCol), _P(MsCol), _P(MsCol), _P(MsCol), _U64, _V,
+                                _V, _V, _P(_U64), _P(_U64), _V, _V]),
     "ms_gpu_set_tuning": (C.c_int, [_P(MsTuning)]),
     "ms_gpu_get_tuning": (C.c_int, [_P(MsTuning)]),
     "ms_gpu_gen_uniform_bits": (C.c_int, [_U64, C.c_uint, _U64, _V, _V]),
@@ -441,6 +443,22 @@ def get_tuning() -> dict:
     t = MsTuning()
     _check(_lib.ms_gpu_get_tuning(C.byref(t)), "get_tuning")
     return {k: getattr(t, k) for k, _ in MsTuning._fields_}
+
+
+def query3(filter_col: Column, cmp: int, c: int, fk: Column, l: Column, gkey: Column, measure: Column,
+           cap: int = 1 << 16, stream=None):
+    """The fused select -> semi_join -> intersect -> project -> group -> sum
+    query.  Returns (keys, extents, sums, |P|) in group-id order."""
+    keys = np.zeros(cap, np.uint64)
+    ext = np.zeros(cap, np.uint64)
+    sums = np.zeros(cap, np.uint64)
+    ng, npos = _U64(), _U64()
+    _check(_lib.ms_gpu_query3(C.byref(filter_col.desc), cmp, c, C.byref(fk.desc), C.byref(l.desc),
+                              C.byref(gkey.desc), C.byref(measure.desc), cap, keys.ctypes.data, ext.ctypes.data,
+                              sums.ctypes.data, C.byref(ng), C.byref(npos), filter_col.arena.h, _stream_ptr(stream)),
+           "query3")
+    k = int(ng.value)
+    return keys[:k], ext[:k], sums[:k], int(npos.value)
 
 
 def device_info():

@@ -214,6 +214,19 @@ int ms_gpu_select_noalloc(int cmp, uint64_t val, const ms_col *in, uint64_t *d_o
                           uint64_t out_capacity, uint64_t *d_out_count, unsigned *d_err, void *stream);
 uint64_t ms_gpu_select_noalloc_max_rows(void);
 
+/* The fused compressed multi-operator query: select(filter cmp c) ->
+ * semi_join(l, fk) -> intersect -> project(gkey, measure) -> group ->
+ * grouped agg_sum, in one pass over the fact table (no counterpart as one
+ * call in the reference; it equals the operator pipeline of
+ * select_compr.h, join_semi_equi_compr.h, intersect_compr.h, project_compr.h,
+ * group_compr.h and scalar/agg_sum_uncompr.h bit for bit).  Outputs, in group
+ * id order (first occurrence): keys, extents (first position within the
+ * intersected position list, as group_vec returns them) and sums. */
+int ms_gpu_query3(const ms_col *filter, int cmp, uint64_t c, const ms_col *fk, const ms_col *l,
+                  const ms_col *gkey, const ms_col *measure, uint64_t cap, uint64_t *h_keys,
+                  uint64_t *h_ext, uint64_t *h_sums, uint64_t *n_groups, uint64_t *n_rows_p,
+                  ms_arena *arena, void *stream);
+
 /* ---- per-block format selection and the learned selector ------------------
  * Blocks of ms_gpu_sel_block_values() = 2048 values; five candidates per block
  * (0 static_vbp<max width>, 1 dynamic_vbp, 2 delta+dvbp, 3 for+dvbp, 4 rle),

@@ -101,3 +101,25 @@ def test_compressed_to_compressed(ms, arena, orc):
     b, m = orc.compress(O.FOR_DVBP, 0, v)
     assert bcol.meta() == m
     assert np.array_equal(bcol.to_numpy(), v)
+
+
+def test_device_generators_match_oracle(ms, arena, orc):
+    """The device generators produce the oracle's columns bit for bit."""
+    import ctypes as C
+    lib = ms.lib()
+    n = 300_007
+    geo = orc.geom_table(0.25)
+    zipf = orc.zipf_table(1.2, 1 << 20)
+    d_geo, d_zipf = arena.alloc(geo.nbytes), arena.alloc(zipf.nbytes)
+    ms._memcpy_h2d(d_geo, geo)
+    ms._memcpy_h2d(d_zipf, zipf)
+    out = arena.alloc(8 * n)
+    checks = [
+        (lambda: lib.ms_gpu_gen_uniform_bits(5, 17, n, out, None), orc.uniform_bits(5, 17, n)),
+        (lambda: lib.ms_gpu_gen_from_table(6, d_zipf, len(zipf), n, out, None), orc.from_table(6, zipf, n)),
+        (lambda: lib.ms_gpu_gen_sorted_gaps(7, d_geo, len(geo), n, out, arena.h, None), orc.sorted_gaps(7, geo, n)),
+        (lambda: lib.ms_gpu_gen_runs(8, 5, 20, n, out, arena.h, None), orc.runs(8, 5, 20, n)),
+    ]
+    for gen, expect in checks:
+        ms._check(gen(), "gen")
+        assert np.array_equal(ms._memcpy_d2h(out, 8 * n).view(np.uint64), expect)
