@@ -308,9 +308,13 @@ def run_gpu(args):
             "clocks": clk.summary(), "e2e": e2e, "gpu_launches": args.steps}
     if args.log2_rows != 28:
         line["config"]["note"] = "reduced size: profiling run, not the benchmark workload"
+    arena.close()
     if not args.no_selector and world == 1:
-        arena.close()
         line["learned_selector"] = selector_run(ms, args)
+    if not args.no_star and world == 1:
+        from engine_b200 import star_query
+        line["star_query"] = star_query.run(args.log2_rows, 5)
+        ok = ok and line["star_query"]["bit_exact"]
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
             line["cpu_baseline"] = cpu_baseline(1)
@@ -321,8 +325,6 @@ def run_gpu(args):
         torch.distributed.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
-    if args.no_selector or world > 1:
-        arena.close()
     return 0 if ok else 1
 
 
@@ -332,10 +334,9 @@ def selector_run(ms, args):
     Zipf data; MLP trained on 2^20 labelled 2048-value blocks (2000 Adam
     steps, batch 4096).  Times are device times (CUDA events) on this GPU."""
     import torch
-    import oracle
     import engine_b200.selector as S
-    orc = oracle.Oracle()
-    zipf = orc.zipf_table(1.2, 1 << 20)
+    from engine_b200.datagen import zipf_table
+    zipf = zipf_table(1.2, 1 << 20)
     stream = torch.cuda.current_stream()
     arena = ms.Arena(20 << 30)
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
@@ -437,7 +438,7 @@ def selector_run(ms, args):
                     ms._check(S._L.ms_gpu_sel_analyze(col, n_eval, st_all, None, sp), "analyze")
                     stp = st_all
                 cont = S.Container(arena, col, n_eval, stp, pick, stream=stream)
-                results[name] = cont.select_sum(oracle.CMP_LT, cmp_val, stream=stream) + (cont.nbytes,)
+                results[name] = cont.select_sum(ms.less, cmp_val, stream=stream) + (cont.nbytes,)
 
             results[name + "_ms"] = timed(e2e, reps=2)
         ok = (results["exhaustive"][:2] == (exp_s, exp_c) and results["learned"][:2] == (exp_s, exp_c)
@@ -532,6 +533,7 @@ def main():
     ap.add_argument("--sel-log2-train", type=int, default=20, help="training blocks = 2^N")
     ap.add_argument("--sel-log2-eval", type=int, default=30, help="evaluation column values = 2^N")
     ap.add_argument("--sel-steps", type=int, default=2000, help="Adam steps")
+    ap.add_argument("--no-star", action="store_true", help="skip the fused star-query leg")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -85,6 +85,8 @@ _sig = {
     "ms_gpu_query3": (C.c_int, [_P(MsCol), C.c_int, _U64, _P(MsCol), _P(MsCol), _P(MsCol), _P(MsCol), _U64, _V,
                                 _V, _V, _P(_U64), _P(_U64), _V, _V]),
     "ms_gpu_set_tuning": (C.c_int, [_P(MsTuning)]),
+    "ms_gpu_set_query_tuning": (C.c_int, [_P(MsTuning)]),
+    "ms_gpu_get_query_tuning": (C.c_int, [_P(MsTuning)]),
     "ms_gpu_get_tuning": (C.c_int, [_P(MsTuning)]),
     "ms_gpu_gen_uniform_bits": (C.c_int, [_U64, C.c_uint, _U64, _V, _V]),
     "ms_gpu_gen_from_table": (C.c_int, [_U64, _V, _U64, _U64, _V, _V]),
@@ -459,6 +461,19 @@ def query3(filter_col: Column, cmp: int, c: int, fk: Column, l: Column, gkey: Co
            "query3")
     k = int(ng.value)
     return keys[:k], ext[:k], sums[:k], int(npos.value)
+
+
+def set_query_tuning(staged: int = 1, warps: int = 16, stages: int = 4, stage_bytes: int = 40960) -> None:
+    """Launch configuration of query3's staged kernel."""
+    t = MsTuning(staged=staged, warps=warps, stages=stages, stage_bytes=stage_bytes, ctas_per_sm=1,
+                 values_per_thread=16)
+    _check(_lib.ms_gpu_set_query_tuning(C.byref(t)), "set_query_tuning")
+
+
+def get_query_tuning() -> dict:
+    t = MsTuning()
+    _check(_lib.ms_gpu_get_query_tuning(C.byref(t)), "get_query_tuning")
+    return {"staged": t.staged, "warps": t.warps, "stages": t.stages, "stage_bytes": t.stage_bytes}
 
 
 def device_info():

@@ -26,17 +26,16 @@ def main():
     import torch
 
     import engine_b200 as ms
-    import oracle
+    from engine_b200.datagen import geom_table, zipf_table
     log2n = int(sys.argv[1]) if len(sys.argv) > 1 else 28
     out_path = sys.argv[2] if len(sys.argv) > 2 else None
     n = 1 << log2n
     lib = ms.lib()
-    orc = oracle.Oracle()
     arena = ms.Arena(24 << 30)
     stream = torch.cuda.current_stream()
     sp = stream.cuda_stream
-    zipf = orc.zipf_table(1.2, 1 << 20)
-    geo = orc.geom_table(0.25)
+    zipf = zipf_table(1.2, 1 << 20)
+    geo = geom_table(0.25)
     d_zipf = arena.alloc(zipf.nbytes)
     ms._memcpy_h2d(d_zipf, zipf)
     d_geo = arena.alloc(geo.nbytes)

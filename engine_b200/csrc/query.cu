@@ -19,8 +19,11 @@
 #include <algorithm>
 #include <vector>
 
+#include "fastpath.cuh"
 #include "internal.h"
 #include "scan.cuh"
+#include "stream.cuh"
+#include "tma.cuh"
 
 namespace ms {
 namespace {
@@ -59,7 +62,7 @@ __device__ __forceinline__ bool gtable_add(const GTable &t, uint64_t key, uint64
 __global__ void __launch_bounds__(256) k_query3(ColView filt, ColView fk, ColView gkey, ColView meas, int cmp,
                                                uint64_t c, const uint32_t *__restrict__ bits, uint64_t lo,
                                                uint64_t span, GTable gt, uint32_t *__restrict__ blk_hits,
-                                               unsigned *err) {
+                                               uint64_t b_begin, unsigned *err) {
     __shared__ unsigned long long s_key[kQSlots], s_first[kQSlots], s_sum[kQSlots];
     for (unsigned i = threadIdx.x; i < kQSlots; i += blockDim.x) {
         s_key[i] = kQEmpty;
@@ -69,7 +72,7 @@ __global__ void __launch_bounds__(256) k_query3(ColView filt, ColView fk, ColVie
     __syncthreads();
     const unsigned lane = threadIdx.x & 31u, l = lane & 7u, q = lane >> 3;
     bool ok = true, fit = true;
-    for (uint64_t b = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) / 32; b < filt.nblocks_total();
+    for (uint64_t b = b_begin + (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) / 32; b < filt.nblocks_total();
          b += uint64_t(gridDim.x) * blockDim.x / 32) {
         uint64_t v[16];
         unsigned valid;
@@ -142,6 +145,282 @@ __global__ void __launch_bounds__(256) k_query3(ColView filt, ColView fk, ColVie
     if (!fit) atomicOr(err, kErrCapacity);
 }
 
+// ---------------------------------------------------------------------------
+// Staged variant.  One persistent CTA per SM: warp 0 forms tiles of
+// consecutive 512-row blocks whose bytes in all four fact columns fit one
+// stage buffer and brings each column's range into shared memory with one
+// bulk copy; consumer warps take the tile's blocks round-robin.  Per block
+// the filter is decoded and compared inside the bit-width switch (all 512
+// rows); the foreign key, group key and measure are not decoded as blocks:
+// only the values of rows still alive are extracted from the staged words
+// (about 10%, 1% and 1% of the rows in the star query), so the consumers stay
+// below the memory time.  Requires the filter in uncompr/static_vbp/
+// dynamic_vbp and the other three columns in those or for_f (delta_f and
+// rows in the uncompressed rests go through k_query3).
+// ---------------------------------------------------------------------------
+constexpr unsigned kQTile = 32;  // blocks per tile (one producer lane each)
+constexpr unsigned kQCols = 4;   // filter, fk, group key, measure
+
+struct QStage {
+    uint64_t b0;
+    unsigned nblk;
+    unsigned pad;
+};
+
+struct QCfg {
+    unsigned stages;
+    unsigned stage_bytes;
+};
+
+// value of slot s (0..63) of lane l in a vbp block of width bw
+__device__ __forceinline__ uint64_t vbp_extract(const uint64_t *blk, unsigned bw, unsigned l, unsigned s) {
+    const unsigned p = s * bw, w = p >> 6, sh = p & 63u;
+    uint64_t x = blk[w * 8u + l] >> sh;
+    if (sh + bw > 64u) x |= blk[(w + 1u) * 8u + l] << (64u - sh);
+    return bw >= 64u ? x : x & ((uint64_t(1) << bw) - 1u);
+}
+
+__host__ __device__ inline uint64_t q3_meta_bytes(unsigned S) {
+    return (uint64_t(16) * S + sizeof(QStage) * S + 5ull * kQCols * S * kQTile + 127) / 128 * 128;
+}
+
+template <int W>
+__global__ void __launch_bounds__(32 * (W + 1), 1)
+    k_query3_tma(ColView fk, ColView gkey, ColView meas, StreamCol c0, StreamCol c1, StreamCol c2, StreamCol c3,
+                 Pred pred, const uint32_t *__restrict__ bits, uint64_t lo, uint64_t span, QCfg cfg, GTable gt,
+                 uint32_t *__restrict__ blk_hits, unsigned *err) {
+    extern __shared__ __align__(128) uint8_t smem[];
+    const unsigned S = cfg.stages, SB = cfg.stage_bytes;
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem);
+    uint64_t *empty = full + S;
+    QStage *desc = reinterpret_cast<QStage *>(empty + S);
+    uint32_t *offs = reinterpret_cast<uint32_t *>(desc + S);                 // [S][kQCols][kQTile]
+    uint8_t *bws = reinterpret_cast<uint8_t *>(offs + S * kQCols * kQTile);  // [S][kQCols][kQTile]
+    uint8_t *ring = smem + q3_meta_bytes(S);
+    unsigned long long *s_key = reinterpret_cast<unsigned long long *>(ring + size_t(S) * SB);
+    unsigned long long *s_first = s_key + kQSlots;
+    unsigned long long *s_sum = s_first + kQSlots;
+
+    const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    for (unsigned i = threadIdx.x; i < kQSlots; i += blockDim.x) {
+        s_key[i] = kQEmpty;
+        s_first[i] = ~0ull;
+        s_sum[i] = 0;
+    }
+    if (threadIdx.x == 0) {
+        for (unsigned st = 0; st < S; st++) {
+            mbar_init(full + st, 1);
+            mbar_init(empty + st, W);
+        }
+        mbar_fence_init();
+    }
+    __syncthreads();
+
+    const uint64_t nbs = minu(minu(c0.nb, c1.nb), minu(c2.nb, c3.nb));
+    const uint64_t b_lo = nbs * blockIdx.x / gridDim.x, b_hi = nbs * (blockIdx.x + 1) / gridDim.x;
+    bool ok = true, fit = true, bad = false;
+
+    if (warp == 0) {
+        // ---------------- producer ----------------
+        const StreamCol *cols[kQCols] = {&c0, &c1, &c2, &c3};
+        uint64_t b = b_lo;
+        unsigned t = 0;
+        for (;; t++) {
+            const unsigned st = t % S, use = t / S;
+            if (use > 0 && !mbar_wait(empty + st, (use - 1) & 1u)) {
+                ok = false;
+                break;
+            }
+            if (b >= b_hi) {
+                if (lane == 0) {
+                    desc[st].nblk = 0;
+                    mbar_arrive(full + st);
+                }
+                t++;
+                break;
+            }
+            const uint64_t blk = b + lane;
+            const bool valid = blk < b_hi;
+            uint64_t off[kQCols], len[kQCols], x0[kQCols];
+            unsigned bw[kQCols];
+            uint64_t need = 0;
+#pragma unroll
+            for (unsigned c = 0; c < kQCols; c++) {
+                off[c] = 0;
+                bw[c] = 0;
+                if (valid) blk_loc(*cols[c], blk, off[c], bw[c]);
+                x0[c] = __shfl_sync(0xFFFFFFFFu, off[c], 0);
+                len[c] = valid ? off[c] + 64ull * bw[c] - x0[c] : 0;
+                need += align_up(len[c], 128);
+            }
+            const bool fits = valid && need <= SB;
+            const unsigned T = __popc(__ballot_sync(0xFFFFFFFFu, fits));
+            if (T == 0) {  // one block larger than a stage: configuration error
+                if (lane == 0) {
+                    atomicOr(err, kErrCapacity);
+                    desc[st].nblk = 0;
+                    mbar_arrive(full + st);
+                }
+                ok = false;
+                t++;
+                break;
+            }
+            uint32_t cbase[kQCols];
+            uint64_t clen[kQCols];
+            uint32_t acc = 0;
+#pragma unroll
+            for (unsigned c = 0; c < kQCols; c++) {
+                clen[c] = __shfl_sync(0xFFFFFFFFu, len[c], T - 1);
+                cbase[c] = acc;
+                acc += uint32_t(align_up(clen[c], 128));
+            }
+            if (lane < T) {
+#pragma unroll
+                for (unsigned c = 0; c < kQCols; c++) {
+                    offs[(st * kQCols + c) * kQTile + lane] = st * SB + cbase[c] + uint32_t(off[c] - x0[c]);
+                    bws[(st * kQCols + c) * kQTile + lane] = uint8_t(bw[c]);
+                }
+            }
+            __syncwarp();
+            if (lane == 0) {
+                __threadfence_block();
+                desc[st].b0 = b;
+                desc[st].nblk = T;
+                __threadfence_block();
+                uint64_t total = 0;
+#pragma unroll
+                for (unsigned c = 0; c < kQCols; c++) total += clen[c];
+                mbar_arrive_expect_tx(full + st, unsigned(total));
+#pragma unroll
+                for (unsigned c = 0; c < kQCols; c++)
+                    bulk_g2s(ring + st * SB + cbase[c], cols[c]->base + x0[c], unsigned(clen[c]), full + st);
+            }
+            __syncwarp();
+            b += T;
+        }
+        const unsigned issued = t;
+        for (unsigned st = 0; st < S && st < issued; st++) {
+            const unsigned uses = (issued - st + S - 1) / S;
+            if (!mbar_wait(full + st, (uses - 1) & 1u)) ok = false;
+        }
+    } else {
+        // ---------------- consumers ----------------
+        const unsigned cw = warp - 1, l = lane & 7u, q = lane >> 3;
+        const bool fk_for = fk.fmt == MS_FMT_FOR_DVBP, g_for = gkey.fmt == MS_FMT_FOR_DVBP,
+                   m_for = meas.fmt == MS_FMT_FOR_DVBP;
+        for (unsigned t = 0;; t++) {
+            const unsigned st = t % S, use = t / S;
+            if (!mbar_wait(full + st, use & 1u)) {
+                ok = false;
+                break;
+            }
+            const unsigned T = desc[st].nblk;
+            if (T == 0) break;
+            const uint64_t b0 = desc[st].b0;
+            const unsigned j0 = unsigned((cw + W - (b0 - b_lo) % W) % W);
+            const uint32_t *o = offs + st * kQCols * kQTile;
+            const uint8_t *w = bws + st * kQCols * kQTile;
+            for (unsigned j = j0; j < T; j += W) {
+                const uint64_t blk = b0 + j;
+                unsigned m = mask_block_rt(w[j], reinterpret_cast<const uint64_t *>(ring + o[j]), l, q, pred, bad);
+                // semi-join probe of the surviving rows
+                if (__any_sync(0xFFFFFFFFu, m != 0)) {
+                    const uint64_t *kb = reinterpret_cast<const uint64_t *>(ring + o[kQTile + j]);
+                    const unsigned kbw = w[kQTile + j];
+                    if (kbw - 1u >= 64u) {
+                        bad = true;
+                        m = 0;
+                    }
+                    const uint64_t kref = fk_for ? __ldg(fk.aux + (blk >> 1)) : 0;
+                    // four probes in flight per thread: the bitmap words are
+                    // requested together, then tested
+                    for (unsigned r = m; r;) {
+                        unsigned kk[4];
+                        uint32_t word[4], bit[4];
+                        bool had[4], inr[4];
+#pragma unroll
+                        for (int i = 0; i < 4; i++) {
+                            had[i] = r != 0;
+                            kk[i] = had[i] ? unsigned(__ffs(r) - 1) : 0u;
+                            r &= r - 1;
+                            const uint64_t v = vbp_extract(kb, kbw, l, 16u * q + kk[i]) + kref;
+                            const uint64_t d = v - lo;
+                            inr[i] = had[i] && v >= lo && d < span;
+                            word[i] = inr[i] ? __ldg(bits + (d >> 5)) : 0u;
+                            bit[i] = unsigned(d & 31u);
+                        }
+#pragma unroll
+                        for (int i = 0; i < 4; i++)
+                            if (had[i] && !(inr[i] && ((word[i] >> bit[i]) & 1u))) m &= ~(1u << kk[i]);
+                    }
+                }
+                unsigned rank[16];
+                const unsigned total = block_ranks(m, l, q, rank);
+                if (lane == 0) blk_hits[blk] = total;
+                if (total == 0) continue;
+                const uint64_t *gb = reinterpret_cast<const uint64_t *>(ring + o[2 * kQTile + j]);
+                const uint64_t *mb = reinterpret_cast<const uint64_t *>(ring + o[3 * kQTile + j]);
+                const unsigned gbw = w[2 * kQTile + j], mbw = w[3 * kQTile + j];
+                if (gbw - 1u >= 64u || mbw - 1u >= 64u) {
+                    bad = true;
+                    continue;
+                }
+                const uint64_t gref = g_for ? __ldg(gkey.aux + (blk >> 1)) : 0;
+                const uint64_t mref = m_for ? __ldg(meas.aux + (blk >> 1)) : 0;
+                const uint64_t row0 = blk * kBlock;
+                for (unsigned r = m; __any_sync(0xFFFFFFFFu, r != 0); r &= r - 1) {
+                    const bool hit = r != 0;
+                    const unsigned hm = __ballot_sync(0xFFFFFFFFu, hit);
+                    if (!hit) continue;
+                    const unsigned k = __ffs(r) - 1;
+                    unsigned rk = 0;
+#pragma unroll
+                    for (unsigned kk = 0; kk < 16; kk++) rk = kk == k ? rank[kk] : rk;
+                    const uint64_t key = vbp_extract(gb, gbw, l, 16u * q + k) + gref;
+                    const uint64_t val = vbp_extract(mb, mbw, l, 16u * q + k) + mref;
+                    const uint64_t first = ((row0 + (16u * q + k) * 8u + l) << 9) | rk;
+                    const unsigned peers = __match_any_sync(hm, key);
+                    uint64_t sm = val, f = first;
+                    for (unsigned rest = peers; rest;) {
+                        const int src = __ffs(rest) - 1;
+                        rest &= rest - 1;
+                        const uint64_t so = __shfl_sync(peers, val, src);
+                        const uint64_t fo = __shfl_sync(peers, first, src);
+                        if (src != int(lane)) {
+                            sm += so;
+                            f = minu(f, fo);
+                        }
+                    }
+                    if (int(lane) != __ffs(peers) - 1) continue;
+                    uint64_t h = qhash(key) & (kQSlots - 1);
+                    bool done = false;
+                    if (key != kQEmpty) {
+                        for (unsigned p = 0; p < 16; p++) {
+                            const unsigned long long old = atomicCAS(s_key + h, kQEmpty, key);
+                            if (old == kQEmpty || old == key) {
+                                atomicMin(s_first + h, (unsigned long long)f);
+                                atomicAdd(s_sum + h, (unsigned long long)sm);
+                                done = true;
+                                break;
+                            }
+                            h = (h + 1) & (kQSlots - 1);
+                        }
+                    }
+                    if (!done) fit &= gtable_add(gt, key, f, sm);
+                }
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(empty + st);
+        }
+    }
+    __syncthreads();
+    for (unsigned i = threadIdx.x; i < kQSlots; i += blockDim.x)
+        if (s_key[i] != kQEmpty) fit &= gtable_add(gt, s_key[i], s_first[i], s_sum[i]);
+    if (!ok) atomicOr(err, kErrTimeout);
+    if (bad) atomicOr(err, kErrCorrupt);
+    if (!fit) atomicOr(err, kErrCapacity);
+}
+
 // bitmap of the build side's keys (dense range)
 __global__ void k_q3_bits(ColView l, uint64_t lo, uint32_t *bits, unsigned *err) {
     const unsigned lane = threadIdx.x & 31u, ll = lane & 7u, q = lane >> 3;
@@ -182,15 +461,52 @@ __global__ void k_minmax_q(ColView c, unsigned long long *mn, unsigned long long
     atomicMax(mx, (unsigned long long)hi);
 }
 
-// extent of every group: hits in earlier blocks + rank within its block
-__global__ void k_q3_extents(GTable gt, const uint64_t *__restrict__ blk_off, unsigned long long *__restrict__ ext,
-                             unsigned long long *__restrict__ row) {
+// extent of every group (hits in earlier blocks + rank within its block),
+// compacted to dense arrays in slot-arrival order
+__global__ void k_q3_extents(GTable gt, const uint64_t *__restrict__ blk_off, unsigned long long *__restrict__ cnt,
+                             uint64_t *__restrict__ o_key, uint64_t *__restrict__ o_ext, uint64_t *__restrict__ o_sum,
+                             uint64_t *__restrict__ o_row) {
     for (uint64_t h = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; h <= gt.mask; h += uint64_t(gridDim.x) * blockDim.x) {
         if (gt.keys[h] == kQEmpty) continue;
         const uint64_t f = gt.first[h];
         const uint64_t r = f >> 9;
-        ext[h] = blk_off[r / kBlock] + (f & 511u);
-        row[h] = r;
+        const unsigned long long i = atomicAdd(cnt, 1ull);
+        o_key[i] = gt.keys[h];
+        o_ext[i] = blk_off[r / kBlock] + (f & 511u);
+        o_sum[i] = gt.sums[h];
+        o_row[i] = r;
+    }
+}
+
+bool random_access(const ColView &v) { return plain(v) || v.fmt == MS_FMT_FOR_DVBP; }
+
+// launch configuration of the staged kernel (consumer warps 8/16/24)
+ms_tuning g_q3 = {1, 16, 4, 40960, 1, 16};
+
+template <int W>
+int launch_q3_tma_w(const ColView &fv, const ColView &kv, const ColView &gv, const ColView &mv, const StreamCol &s0,
+                    const StreamCol &s1, const StreamCol &s2, const StreamCol &s3, const Pred &pred,
+                    const uint32_t *bits, uint64_t lo, uint64_t span, const GTable &gt, uint32_t *hits,
+                    unsigned *d_err, cudaStream_t st) {
+    const QCfg cfg{g_q3.stages, g_q3.stage_bytes};
+    const size_t shm = q3_meta_bytes(cfg.stages) + size_t(cfg.stages) * cfg.stage_bytes + 3ull * 8 * kQSlots;
+    auto kern = k_query3_tma<W>;
+    MS_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
+    kern<<<unsigned(sm_count()), 32 * (W + 1), shm, st>>>(kv, gv, mv, s0, s1, s2, s3, pred, bits, lo, span, cfg,
+                                                          gt, hits, d_err);
+    MS_CUDA_TRY(cudaGetLastError());
+    (void)fv;
+    return MS_OK;
+}
+
+int launch_q3_tma(const ColView &fv, const ColView &kv, const ColView &gv, const ColView &mv, const StreamCol &s0,
+                  const StreamCol &s1, const StreamCol &s2, const StreamCol &s3, const Pred &pred,
+                  const uint32_t *bits, uint64_t lo, uint64_t span, const GTable &gt, uint32_t *hits,
+                  unsigned *d_err, cudaStream_t st) {
+    switch (g_q3.warps) {
+    case 8: return launch_q3_tma_w<8>(fv, kv, gv, mv, s0, s1, s2, s3, pred, bits, lo, span, gt, hits, d_err, st);
+    case 24: return launch_q3_tma_w<24>(fv, kv, gv, mv, s0, s1, s2, s3, pred, bits, lo, span, gt, hits, d_err, st);
+    default: return launch_q3_tma_w<16>(fv, kv, gv, mv, s0, s1, s2, s3, pred, bits, lo, span, gt, hits, d_err, st);
     }
 }
 
@@ -198,6 +514,28 @@ __global__ void k_q3_extents(GTable gt, const uint64_t *__restrict__ blk_off, un
 }  // namespace ms
 
 using namespace ms;
+
+// Launch configuration of the fused query's staged kernel: staged (0 = the
+// direct kernel only), warps (consumer warps: 8, 16 or 24), stages and
+// stage_bytes (shared-memory ring; stages x stage_bytes + 48 KiB group table
+// must fit 227 KiB).  The other fields are ignored.
+extern "C" int ms_gpu_set_query_tuning(const ms_tuning *t) {
+    if (!t) return ms_fail(MS_ERR_INVALID, "set_query_tuning: null");
+    if (t->warps != 8 && t->warps != 16 && t->warps != 24)
+        return ms_fail(MS_ERR_INVALID, "set_query_tuning: warps must be 8, 16 or 24");
+    if (t->stages < 2 || t->stages > 16 || t->stage_bytes % 128 || t->stage_bytes < 16384)
+        return ms_fail(MS_ERR_INVALID, "set_query_tuning: stages in 2..16, stage_bytes a multiple of 128, >= 16 KiB");
+    if (q3_meta_bytes(t->stages) + uint64_t(t->stages) * t->stage_bytes + 3ull * 8 * kQSlots > 232448)
+        return ms_fail(MS_ERR_INVALID, "set_query_tuning: shared memory above 227 KiB");
+    g_q3 = *t;
+    return MS_OK;
+}
+
+extern "C" int ms_gpu_get_query_tuning(ms_tuning *t) {
+    if (!t) return ms_fail(MS_ERR_INVALID, "get_query_tuning: null");
+    *t = g_q3;
+    return MS_OK;
+}
 
 // The fused query.  Outputs (host arrays of capacity `cap`): group keys, the
 // group extents (first position of each group within P, as group_vec
@@ -212,6 +550,7 @@ extern "C" int ms_gpu_query3(const ms_col *filter, int cmp, uint64_t c, const ms
     if (fk->count_values != n || gkey->count_values != n || measure->count_values != n)
         return ms_fail(MS_ERR_INVALID, "query3: fact columns differ in length");
     cudaStream_t st = (cudaStream_t)stream;
+    const uint64_t mark0 = a->used;  // everything below is scratch
     ColView fv, kv, gv, mv, lv;
     int rc;
     if ((rc = prepare_view(filter, a, st, &fv)) || (rc = prepare_view(fk, a, st, &kv)) ||
@@ -234,59 +573,100 @@ extern "C" int ms_gpu_query3(const ms_col *filter, int cmp, uint64_t c, const ms
     uint64_t lo = 0, span = 0;
     if (lv.n) {
         lo = hmm[0];
+        if (hmm[1] - hmm[0] >= (uint64_t(1) << 30))
+            return ms_fail(MS_ERR_UNSUPPORTED, "query3: build keys span more than 2^30");
         span = hmm[1] - hmm[0] + 1;
-        if (span > (uint64_t(1) << 30)) return ms_fail(MS_ERR_UNSUPPORTED, "query3: build keys span more than 2^30");
     }
     const uint64_t words = (span + 31) / 32 + 1;
     uint32_t *bits = arena_take_t<uint32_t>(a, words);
-    const uint64_t nbt = fv.nblocks_total();
-    uint32_t *hits = arena_take_t<uint32_t>(a, nbt + 1);
-    uint64_t *boff = arena_take_t<uint64_t>(a, nbt + 1);
-    uint64_t *tot = arena_take_t<uint64_t>(a, 1);
-    uint64_t *scr = arena_take_t<uint64_t>(a, scan_scratch_words(nbt, 1));
-    const uint64_t slots = 1 << 16;
-    GTable gt{arena_take_t<unsigned long long>(a, slots), arena_take_t<unsigned long long>(a, slots),
-              arena_take_t<unsigned long long>(a, slots), slots - 1};
-    unsigned long long *ext = arena_take_t<unsigned long long>(a, slots);
-    unsigned long long *row = arena_take_t<unsigned long long>(a, slots);
-    if (!bits || !hits || !boff || !tot || !scr || !gt.keys || !gt.first || !gt.sums || !ext || !row)
-        return ms_fail(MS_ERR_NOMEM, "arena exhausted (query3)");
+    if (!bits) return ms_fail(MS_ERR_NOMEM, "arena exhausted (query3)");
     MS_CUDA_TRY(cudaMemsetAsync(bits, 0, 4 * words, st));
-    MS_CUDA_TRY(cudaMemsetAsync(gt.keys, 0xFF, 8 * slots, st));
-    MS_CUDA_TRY(cudaMemsetAsync(gt.first, 0xFF, 8 * slots, st));
-    MS_CUDA_TRY(cudaMemsetAsync(gt.sums, 0, 8 * slots, st));
     if (lv.n) {
         k_q3_bits<<<grid, 256, 0, st>>>(lv, lo, bits, a->d_err);
         MS_CUDA_TRY(cudaGetLastError());
     }
-    if (nbt) {
-        const unsigned g2 = unsigned(maxu(1, minu((nbt + 7) / 8, persistent_grid(256, 4))));
-        k_query3<<<g2, 256, 0, st>>>(fv, kv, gv, mv, cmp, c, bits, lo, span, gt, hits, a->d_err);
-        MS_CUDA_TRY(cudaGetLastError());
-        MS_CUDA_TRY((scan_exclusive<uint32_t, 1>(hits, nbt, boff, tot, scr, st)));
-        k_q3_extents<<<64, 256, 0, st>>>(gt, boff, ext, row);
-        MS_CUDA_TRY(cudaGetLastError());
+    const uint64_t nbt = fv.nblocks_total();
+    // The global group table starts at 2^16 slots and grows by 16x (up to
+    // 2^24) when it fills, re-running the pass.
+    uint64_t slots = uint64_t(1) << 16;
+    std::vector<uint64_t> k, e, s, r;
+    uint64_t ng = 0, np = 0;
+    for (;;) {
+        const uint64_t mark = a->used;
+        uint32_t *hits = arena_take_t<uint32_t>(a, nbt + 1);
+        uint64_t *boff = arena_take_t<uint64_t>(a, nbt + 1);
+        uint64_t *tot = arena_take_t<uint64_t>(a, 1);
+        uint64_t *scr = arena_take_t<uint64_t>(a, scan_scratch_words(nbt, 1));
+        GTable gt{arena_take_t<unsigned long long>(a, slots), arena_take_t<unsigned long long>(a, slots),
+                  arena_take_t<unsigned long long>(a, slots), slots - 1};
+        unsigned long long *cnt = arena_take_t<unsigned long long>(a, 1);
+        uint64_t *out = arena_take_t<uint64_t>(a, 4 * slots);
+        if (!hits || !boff || !tot || !scr || !gt.keys || !gt.first || !gt.sums || !cnt || !out)
+            return ms_fail(MS_ERR_NOMEM, "arena exhausted (query3)");
+        MS_CUDA_TRY(cudaMemsetAsync(gt.keys, 0xFF, 8 * slots, st));
+        MS_CUDA_TRY(cudaMemsetAsync(gt.first, 0xFF, 8 * slots, st));
+        MS_CUDA_TRY(cudaMemsetAsync(gt.sums, 0, 8 * slots, st));
+        MS_CUDA_TRY(cudaMemsetAsync(cnt, 0, 8, st));
+        MS_CUDA_TRY(cudaMemsetAsync(tot, 0, 8, st));
+        if (nbt) {
+            uint64_t nbs = 0;  // blocks through the staged kernel
+            if (g_q3.staged && plain(fv) && random_access(kv) && random_access(gv) && random_access(mv)) {
+                const StreamCol s0 = stream_of(fv), s1 = stream_of(kv), s2 = stream_of(gv), s3 = stream_of(mv);
+                nbs = minu(minu(s0.nb, s1.nb), minu(s2.nb, s3.nb));
+                if (nbs) {
+                    rc = launch_q3_tma(fv, kv, gv, mv, s0, s1, s2, s3, make_pred(cmp, c), bits, lo, span, gt, hits,
+                                       a->d_err, st);
+                    if (rc) return rc;
+                }
+            }
+            if (nbt > nbs) {
+                const unsigned g2 = unsigned(maxu(1, minu((nbt - nbs + 7) / 8, persistent_grid(256, 4))));
+                k_query3<<<g2, 256, 0, st>>>(fv, kv, gv, mv, cmp, c, bits, lo, span, gt, hits, nbs, a->d_err);
+                MS_CUDA_TRY(cudaGetLastError());
+            }
+            MS_CUDA_TRY((scan_exclusive<uint32_t, 1>(hits, nbt, boff, tot, scr, st)));
+            k_q3_extents<<<unsigned(minu(slots / 256, 1024)), 256, 0, st>>>(gt, boff, cnt, out, out + slots,
+                                                                          out + 2 * slots, out + 3 * slots);
+            MS_CUDA_TRY(cudaGetLastError());
+        }
+        unsigned herr = 0;
+        uint64_t hc[2] = {0, 0};
+        MS_CUDA_TRY(cudaMemcpyAsync(&herr, a->d_err, sizeof herr, cudaMemcpyDeviceToHost, st));
+        MS_CUDA_TRY(cudaMemcpyAsync(hc, cnt, 8, cudaMemcpyDeviceToHost, st));
+        MS_CUDA_TRY(cudaMemcpyAsync(hc + 1, tot, 8, cudaMemcpyDeviceToHost, st));
+        MS_CUDA_TRY(cudaStreamSynchronize(st));
+        if (herr == kErrCapacity && slots < (uint64_t(1) << 24)) {
+            MS_CUDA_TRY(cudaMemsetAsync(a->d_err, 0, sizeof herr, st));
+            a->used = mark;
+            slots <<= 4;
+            continue;
+        }
+        rc = read_err(a, st);
+        if (rc) return rc;
+        ng = hc[0];
+        np = hc[1];
+        k.resize(ng);
+        e.resize(ng);
+        s.resize(ng);
+        r.resize(ng);
+        if (ng) {
+            MS_CUDA_TRY(cudaMemcpyAsync(k.data(), out, 8 * ng, cudaMemcpyDeviceToHost, st));
+            MS_CUDA_TRY(cudaMemcpyAsync(e.data(), out + slots, 8 * ng, cudaMemcpyDeviceToHost, st));
+            MS_CUDA_TRY(cudaMemcpyAsync(s.data(), out + 2 * slots, 8 * ng, cudaMemcpyDeviceToHost, st));
+            MS_CUDA_TRY(cudaMemcpyAsync(r.data(), out + 3 * slots, 8 * ng, cudaMemcpyDeviceToHost, st));
+            MS_CUDA_TRY(cudaStreamSynchronize(st));
+        }
+        break;
     }
-    rc = read_err(a, st);
-    if (rc) return rc;
-    // collect on the host (at most `slots` groups) and order by first row
-    std::vector<uint64_t> k(slots), e(slots), s(slots), r(slots);
-    uint64_t np = 0;
-    if (nbt) {
-        MS_CUDA_TRY(cudaMemcpy(k.data(), gt.keys, 8 * slots, cudaMemcpyDeviceToHost));
-        MS_CUDA_TRY(cudaMemcpy(e.data(), ext, 8 * slots, cudaMemcpyDeviceToHost));
-        MS_CUDA_TRY(cudaMemcpy(s.data(), gt.sums, 8 * slots, cudaMemcpyDeviceToHost));
-        MS_CUDA_TRY(cudaMemcpy(r.data(), row, 8 * slots, cudaMemcpyDeviceToHost));
-        MS_CUDA_TRY(cudaMemcpy(&np, tot, 8, cudaMemcpyDeviceToHost));
-    }
-    std::vector<uint64_t> idx;
-    for (uint64_t h = 0; h < (nbt ? slots : 0); h++)
-        if (k[h] != kQEmpty) idx.push_back(h);
+    a->used = mark0;
+    // group ids follow the first occurrence: order by first row
+    std::vector<uint64_t> idx(ng);
+    for (uint64_t i = 0; i < ng; i++) idx[i] = i;
     std::sort(idx.begin(), idx.end(), [&](uint64_t x, uint64_t y) { return r[x] < r[y]; });
-    *n_groups = idx.size();
+    *n_groups = ng;
     if (n_rows_p) *n_rows_p = np;
-    if (idx.size() > cap) return ms_fail(MS_ERR_NOMEM, "query3: more groups than the output capacity");
-    for (size_t i = 0; i < idx.size(); i++) {
+    if (ng > cap) return ms_fail(MS_ERR_NOMEM, "query3: more groups than the output capacity");
+    for (uint64_t i = 0; i < ng; i++) {
         if (h_keys) h_keys[i] = k[idx[i]];
         if (h_ext) h_ext[i] = e[idx[i]];
         if (h_sums) h_sums[i] = s[idx[i]];

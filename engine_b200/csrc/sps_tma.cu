@@ -20,6 +20,7 @@
 // leaves after the producer has waited for its own copies.
 #include "fastpath.cuh"
 #include "internal.h"
+#include "stream.cuh"
 #include "tma.cuh"
 
 namespace ms {
@@ -27,29 +28,11 @@ namespace {
 
 constexpr unsigned kMaxTile = 32;  // blocks per tile (one producer lane each)
 
-struct StreamCol {
-    const uint8_t *base;
-    const uint64_t *index;  // nullptr: fixed width
-    unsigned fixed_bw;
-    uint64_t nb;            // blocks available to the pipeline
-};
-
 struct TmaCfg {
     unsigned stages;
     unsigned stage_bytes;
     unsigned max_tile;
 };
-
-__device__ __forceinline__ void blk_loc(const StreamCol &c, uint64_t b, uint64_t &off, unsigned &bw) {
-    if (c.index) {
-        const uint64_t e = __ldg(c.index + b);
-        off = idx_off(e);
-        bw = idx_bw(e);
-    } else {
-        bw = c.fixed_bw;
-        off = b * 64ull * bw;
-    }
-}
 
 struct StageDesc {
     uint64_t b0;
@@ -312,28 +295,6 @@ __global__ void __launch_bounds__(256) k_sps_tail(ColView x, ColView y, int cmp,
         if (d_sum) atomicAdd(d_sum, (unsigned long long)s_sum);
         if (d_cnt) atomicAdd(d_cnt, (unsigned long long)s_cnt);
     }
-}
-
-StreamCol stream_of(const ColView &v) {
-    StreamCol s{};
-    if (v.fmt == MS_FMT_UNCOMPR) {
-        s.base = reinterpret_cast<const uint8_t *>(v.rest);
-        s.fixed_bw = 64;  // an uncompressed 512-row block is laid out as vbp_l<64,8>
-        s.nb = v.n / kBlock;
-    } else if (v.fmt == MS_FMT_STATIC_VBP) {
-        s.base = v.data;
-        s.fixed_bw = v.bw;
-        s.nb = v.nb();
-    } else {
-        s.base = v.data;
-        s.index = v.index;
-        s.nb = v.nb();
-    }
-    return s;
-}
-
-bool plain(const ColView &v) {
-    return v.fmt == MS_FMT_UNCOMPR || v.fmt == MS_FMT_STATIC_VBP || v.fmt == MS_FMT_DYNAMIC_VBP;
 }
 
 template <int W, bool kHasY, bool kFast, int VPT>

@@ -226,6 +226,12 @@ int ms_gpu_query3(const ms_col *filter, int cmp, uint64_t c, const ms_col *fk, c
                   const ms_col *gkey, const ms_col *measure, uint64_t cap, uint64_t *h_keys,
                   uint64_t *h_ext, uint64_t *h_sums, uint64_t *n_groups, uint64_t *n_rows_p,
                   ms_arena *arena, void *stream);
+/* Launch configuration of ms_gpu_query3's staged kernel (no counterpart in
+ * the reference): staged (0 = direct kernel only), warps (consumer warps 8,
+ * 16 or 24), stages, stage_bytes; other fields ignored.  Rejects a ring that
+ * does not fit shared memory with the 48 KiB group table. */
+int ms_gpu_set_query_tuning(const ms_tuning *t);
+int ms_gpu_get_query_tuning(ms_tuning *t);
 
 /* ---- per-block format selection and the learned selector ------------------
  * Blocks of ms_gpu_sel_block_values() = 2048 values; five candidates per block
