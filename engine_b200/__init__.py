@@ -86,6 +86,14 @@ _sig = {
                                 _V, _V, _P(_U64), _P(_U64), _V, _V]),
     "ms_gpu_set_tuning": (C.c_int, [_P(MsTuning)]),
     "ms_gpu_set_query_tuning": (C.c_int, [_P(MsTuning)]),
+    "ms_gpu_col_compact": (C.c_int, [_P(MsCol), _P(MsCol), _V, _V]),
+    "ms_gpu_batch_create": (C.c_int, [_P(MsCol), _V, _U64, C.c_int, _V, _P(_V), _V]),
+    "ms_gpu_batch_set_config": (C.c_int, [_V, _P(MsTuning)]),
+    "ms_gpu_batch_get_config": (C.c_int, [_V, _P(MsTuning)]),
+    "ms_gpu_batch_run": (C.c_int, [_V, _V, _V, _V]),
+    "ms_gpu_batch_run_graph": (C.c_int, [_V, _V, _V, _V]),
+    "ms_gpu_batch_info": (C.c_int, [_V, _P(_U64), _P(_U64)]),
+    "ms_gpu_batch_destroy": (None, [_V]),
     "ms_gpu_get_query_tuning": (C.c_int, [_P(MsTuning)]),
     "ms_gpu_get_tuning": (C.c_int, [_P(MsTuning)]),
     "ms_gpu_gen_uniform_bits": (C.c_int, [_U64, C.c_uint, _U64, _V, _V]),
@@ -318,6 +326,14 @@ class Column:
             _memcpy_h2d(pa, aux)
             self.desc.index_aux = pa
 
+    def compact(self, arena: "Arena | None" = None, stream=None) -> "Column":
+        """A copy of this column in storage of exactly its used size."""
+        arena = arena or self.arena
+        out = MsCol()
+        _check(_lib.ms_gpu_col_compact(C.byref(self.desc), C.byref(out), arena.h, _stream_ptr(stream)),
+               "col_compact")
+        return Column(out, arena)
+
     def build_index(self, stream=None) -> None:
         _check(_lib.ms_gpu_build_index(C.byref(self.desc), self.arena.h, _stream_ptr(stream)), "build_index")
 
@@ -474,6 +490,70 @@ def get_query_tuning() -> dict:
     t = MsTuning()
     _check(_lib.ms_gpu_get_query_tuning(C.byref(t)), "get_query_tuning")
     return {"staged": t.staged, "warps": t.warps, "stages": t.stages, "stage_bytes": t.stage_bytes}
+
+
+class Batch:
+    """Many columns, one persistent launch: for every column i,
+    decompress -> select(value cmp consts[i]) -> sum of the selected values.
+    run() returns (counts, sums) as uint64 arrays; graph=True replays a CUDA
+    graph captured on first use."""
+
+    def __init__(self, cols, consts, cmp: int = less, arena: "Arena | None" = None, stream=None):
+        self.cols = list(cols)
+        self.arena = arena or (self.cols[0].arena if self.cols else default_arena())
+        n = len(self.cols)
+        descs = (MsCol * max(n, 1))(*[c.desc for c in self.cols])
+        cv = np.ascontiguousarray(consts, dtype=np.uint64)
+        if len(cv) != n:
+            raise ValueError("one constant per column")
+        self.n = n
+        self.h = _V()
+        _check(_lib.ms_gpu_batch_create(descs, cv.ctypes.data if n else None, n, cmp, self.arena.h,
+                                        C.byref(self.h), _stream_ptr(stream)), "batch_create")
+        self.d_cnt = self.arena.alloc(8 * max(n, 1))
+        self.d_sum = self.arena.alloc(8 * max(n, 1))
+
+    def set_config(self, warps: int = 12, stages: int = 2, stage_bytes: int = 8192, ctas_per_sm: int = 1) -> None:
+        t = MsTuning(staged=1, warps=warps, stages=stages, stage_bytes=stage_bytes, ctas_per_sm=ctas_per_sm,
+                     values_per_thread=16)
+        _check(_lib.ms_gpu_batch_set_config(self.h, C.byref(t)), "batch_set_config")
+
+    def get_config(self) -> dict:
+        t = MsTuning()
+        _check(_lib.ms_gpu_batch_get_config(self.h, C.byref(t)), "batch_get_config")
+        return {"warps": t.warps, "stages": t.stages, "stage_bytes": t.stage_bytes, "ctas_per_sm": t.ctas_per_sm}
+
+    def launch(self, graph: bool = False, stream=None) -> None:
+        f = _lib.ms_gpu_batch_run_graph if graph else _lib.ms_gpu_batch_run
+        _check(f(self.h, self.d_cnt, self.d_sum, _stream_ptr(stream)), "batch_run")
+
+    def results(self):
+        self.arena.check()
+        if not self.n:
+            return np.zeros(0, np.uint64), np.zeros(0, np.uint64)
+        cnt = _memcpy_d2h(self.d_cnt, 8 * self.n).view(np.uint64)
+        s = _memcpy_d2h(self.d_sum, 8 * self.n).view(np.uint64)
+        return cnt, s
+
+    def run(self, graph: bool = False, stream=None):
+        self.launch(graph, stream)
+        return self.results()
+
+    def info(self) -> dict:
+        a, b = _U64(), _U64()
+        _check(_lib.ms_gpu_batch_info(self.h, C.byref(a), C.byref(b)), "batch_info")
+        return {"items": int(a.value), "plan_bytes": int(b.value)}
+
+    def close(self) -> None:
+        if self.h:
+            _lib.ms_gpu_batch_destroy(self.h)
+            self.h = _V()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def device_info():

@@ -1,0 +1,606 @@
+// batch.cu -- many columns, one persistent launch.
+//
+// A batch plan turns a set of columns (any format, any length) into a device
+// work queue of items: up to 32 consecutive 512-row blocks of one column
+// (static_vbp / dynamic_vbp, for_f, delta_f), up to 4096 rows of a column's
+// uncompressed rest, or up to 1024 runs of an rle_f column.  Every column
+// runs decompress -> select(value cmp c_i) -> agg_sum of the selected values
+// (count and sum per column), the per-column chain of the reference's
+// morph / select / agg_sum operators.
+//
+// The kernel is persistent (one or more CTAs per SM) and every warp works
+// alone: it takes the next item off the queue with one atomic, and runs its
+// own S-stage shared-memory ring -- lane 0 issues a 1-D bulk copy (TMA) of the
+// next tile (the consecutive blocks of the item that fit a stage, page headers
+// included) while the warp decodes the previous one.  Items of very different
+// sizes and formats therefore need no cross-warp synchronisation, and a warp
+// keeps S tiles in flight, which is what hides HBM latency.  Blocks are
+// decoded as in the single-column kernels: plain vbp blocks compare and sum
+// inside the bit-width switch, for_f adds the 1024-block reference, delta_f
+// runs the lane-wise prefix with a carry kept in registers across the item's
+// blocks; the carry into an item's first block is a per-item seek value the
+// plan computes once (the values before the item, lane by lane), so items of
+// one column are independent.  The queue is ordered by decoder (kind, bit
+// width), so the warps of an SM mostly run the same instructions.
+//
+// All waits are bounded; errors go to the arena's error word.  The run is a
+// fixed sequence of stream operations (three memsets and one launch) with no
+// host synchronisation, so it can be captured into a CUDA graph; the plan
+// keeps one graph per pair of output buffers.
+#include <algorithm>
+#include <vector>
+
+#include "fastpath.cuh"
+#include "internal.h"
+#include "tma.cuh"
+
+namespace ms {
+namespace {
+
+constexpr unsigned kBItemBlocks = 32;  // blocks per item (one lane each)
+constexpr unsigned kBItemRest = 4096;  // rows of an uncompressed rest per item
+constexpr unsigned kBItemRuns = 1024;  // runs of an rle_f column per item
+
+enum : uint32_t { kItVbp = 0, kItFor = 1, kItDelta = 2, kItRest = 3, kItRle = 4 };
+
+struct BCol {
+    const uint8_t *data;    // compressed blocks (vbp family) or (value, length) pairs (rle_f)
+    const uint64_t *index;  // block index (nullptr: static_vbp, fixed bw)
+    const uint64_t *aux;    // for_f references per 1024-block
+    const uint64_t *rest;   // uncompressed rest rows [n_compr, n)
+    uint64_t n, n_compr, sfrom;
+    uint64_t c;             // comparison constant
+    Pred pred;              // c reduced to a threshold for plain vbp blocks
+    unsigned bw;            // static_vbp width
+    unsigned cf;            // comparison as bits: 1 = less passes, 2 = equal passes, 4 = negate
+};
+
+struct BItem {
+    uint32_t col, kind;
+    uint64_t start;       // first block / first rest row / first run
+    uint32_t count, pad;  // blocks / rows / runs
+    uint64_t seek;        // delta_f: carry slot; rle_f: first row of the item
+};
+
+struct BStage {  // one stage of a warp's ring
+    uint32_t item, nblk;
+    uint64_t b0;
+    uint32_t off[kBItemBlocks];
+    uint8_t bw[kBItemBlocks];
+};
+
+// The comparison without a branch on its kind: (lt & less-passes) |
+// (eq & equal-passes), negated for greater / greaterequal.
+inline unsigned cmp_flags(int cmp) {
+    switch (cmp) {
+    case MS_CMP_EQ: return 2u;
+    case MS_CMP_LT: return 1u;
+    case MS_CMP_LE: return 3u;
+    case MS_CMP_GT: return 7u;
+    default: return 5u;
+    }
+}
+
+__device__ __forceinline__ bool cmp_bits(uint64_t v, uint64_t c, unsigned cf, bool sgn) {
+    const bool lt = sgn ? (int64_t)v < (int64_t)c : v < c;
+    const unsigned hit = ((lt ? 1u : 0u) | (v == c ? 2u : 0u)) & cf & 3u;
+    return (hit ? 1u : 0u) ^ (cf >> 2);
+}
+
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__host__ __device__ inline unsigned bwarp_meta_bytes(unsigned S) {
+    return (8u * S + unsigned(sizeof(BStage)) * S + 127u) / 128u * 128u;
+}
+
+template <int W>
+__global__ void __launch_bounds__(32 * W, 1)
+    k_batch(const BCol *__restrict__ cols, const BItem *__restrict__ items, uint64_t n_items,
+            const uint64_t *__restrict__ seeks, unsigned S, unsigned SBw, unsigned long long *head,
+            unsigned long long *__restrict__ out_cnt, unsigned long long *__restrict__ out_sum, unsigned *err) {
+    extern __shared__ __align__(128) uint8_t smem[];
+    const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31u, l = lane & 7u, q = lane >> 3;
+    uint8_t *mine = smem + size_t(warp) * (bwarp_meta_bytes(S) + size_t(S) * SBw);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(mine);
+    BStage *stg = reinterpret_cast<BStage *>(mine + 8u * S);
+    uint8_t *ring = mine + bwarp_meta_bytes(S);
+    if (lane == 0) {
+        for (unsigned s = 0; s < S; s++) mbar_init(bar + s, 1);
+        mbar_fence_init();
+    }
+    __syncwarp();
+
+    bool ok = true, bad = false;
+    // producer state
+    bool exhausted = false;
+    uint32_t it = 0, it_col = 0;
+    uint64_t it_start = 0, it_next = 0, it_left = 0;
+    uint64_t it_off = 0;  // lane i: byte offset of the item's block i
+    unsigned it_bw = 0;   // lane i: its bit width
+    const uint8_t *it_data = nullptr;
+    unsigned issued = 0, consumed = 0;
+    // consumer state: delta carry of lane l (threads (l, q) all hold it)
+    uint64_t carry = 0;
+
+    auto issue = [&]() {
+        if (it_left == 0) {
+            unsigned long long id = 0;
+            if (lane == 0) id = atomicAdd(head, 1ull);
+            id = __shfl_sync(0xFFFFFFFFu, id, 0);
+            if (id >= n_items) {
+                exhausted = true;
+                return;
+            }
+            it = uint32_t(id);
+            const BItem bi = items[id];
+            it_col = bi.col;
+            if (bi.kind == kItRest || bi.kind == kItRle) {  // read in place: no copy
+                const unsigned s = issued % S;
+                if (lane == 0) {
+                    stg[s].item = it;
+                    stg[s].nblk = 0;
+                    stg[s].b0 = bi.start;
+                    mbar_arrive(bar + s);
+                }
+                __syncwarp();
+                issued++;
+                return;
+            }
+            it_start = it_next = bi.start;
+            it_left = bi.count;
+            // the item's block locations, one lane per block, kept for all its tiles
+            const BCol &c = cols[it_col];
+            it_data = c.data;
+            it_off = 0;
+            it_bw = 0;
+            if (lane < it_left) {
+                if (c.index) {
+                    const uint64_t e = __ldg(c.index + bi.start + lane);
+                    it_off = idx_off(e);
+                    it_bw = idx_bw(e);
+                } else {
+                    it_bw = c.bw;
+                    it_off = (bi.start + lane) * 64ull * c.bw;
+                }
+            }
+        }
+        const unsigned s = issued % S;
+        const unsigned k0 = unsigned(it_next - it_start);  // first block of the tile within the item
+        const bool valid = lane < it_left;
+        const uint64_t off = __shfl_sync(0xFFFFFFFFu, it_off, (k0 + lane) & 31u);
+        const unsigned bw = __shfl_sync(0xFFFFFFFFu, it_bw, (k0 + lane) & 31u);
+        const uint64_t x0 = __shfl_sync(0xFFFFFFFFu, off, 0);
+        const uint64_t len = valid ? off + 64ull * bw - x0 : 0;
+        const bool fits = valid && bw >= 1 && bw <= 64 && len <= SBw;
+        const unsigned fb = __ballot_sync(0xFFFFFFFFu, fits);
+        const unsigned T = fb == 0xFFFFFFFFu ? 32u : unsigned(__ffs(~fb) - 1);  // leading lanes that fit
+        if (T == 0) {  // corrupt width or a block larger than a stage: drop the item
+            if (lane == 0) atomicOr(err, kErrCorrupt);
+            it_left = 0;
+            return;
+        }
+        const uint64_t tl = __shfl_sync(0xFFFFFFFFu, len, T - 1);
+        if (lane < T) {
+            stg[s].off[lane] = uint32_t(off - x0);
+            stg[s].bw[lane] = uint8_t(bw);
+        }
+        if (lane == 0) {
+            stg[s].item = it;
+            stg[s].nblk = T;
+            stg[s].b0 = it_next;
+        }
+        __syncwarp();
+        if (lane == 0) {
+            fence_proxy_async();  // the stage's previous contents were read through the generic proxy
+            mbar_arrive_expect_tx(bar + s, unsigned(tl));
+            bulk_g2s(ring + size_t(s) * SBw, it_data + x0, unsigned(tl), bar + s);
+        }
+        __syncwarp();
+        it_next += T;
+        it_left -= T;
+        issued++;
+    };
+
+    for (;;) {
+        while (!exhausted && issued - consumed < S) issue();
+        if (consumed == issued) break;
+        const unsigned s = consumed % S;
+        if (!mbar_wait(bar + s, (consumed / S) & 1u)) {
+            ok = false;
+            break;
+        }
+        const BStage &sd = stg[s];
+        const BItem bi = items[sd.item];
+        const BCol &c = cols[bi.col];
+        const uint8_t *base = ring + size_t(s) * SBw;
+        uint64_t cnt = 0, sum = 0;
+        if (bi.kind == kItVbp) {
+            for (unsigned j = 0; j < sd.nblk; j++) {
+                const uint64_t *blk = reinterpret_cast<const uint64_t *>(base + sd.off[j]);
+                unsigned k = 0;
+                sum += self_sum_block_rt(sd.bw[j], blk, l, q, c.pred, k, bad);
+                cnt += k;
+            }
+        } else if (bi.kind == kItFor || bi.kind == kItDelta) {
+            if (bi.kind == kItDelta && sd.b0 == bi.start) carry = __ldg(seeks + bi.seek * 8 + l);
+            for (unsigned j = 0; j < sd.nblk; j++) {
+                uint64_t v[16];
+                bad |= !vbp_decode16_rt<true>(sd.bw[j], reinterpret_cast<const uint64_t *>(base + sd.off[j]), l, q, v);
+                if (bi.kind == kItFor) {
+                    const uint64_t ref = __ldg(c.aux + ((sd.b0 + j) >> 1));
+#pragma unroll
+                    for (int k = 0; k < 16; k++) v[k] += ref;
+                } else {
+#pragma unroll
+                    for (int k = 1; k < 16; k++) v[k] += v[k - 1];
+                    const uint64_t tot = v[15];
+                    const uint64_t up = __shfl_up_sync(0xFFFFFFFFu, tot, 8);
+                    uint64_t pre = q >= 1 ? up : 0;
+                    const uint64_t up2 = __shfl_up_sync(0xFFFFFFFFu, tot + pre, 16);
+                    pre += (q >= 2 ? up2 : 0) + carry;
+#pragma unroll
+                    for (int k = 0; k < 16; k++) v[k] += pre;
+                    carry = __shfl_sync(0xFFFFFFFFu, v[15], int(24 + l));  // lane l's last value
+                }
+                // every row of the compressed part precedes the scalar remainder
+#pragma unroll
+                for (int k = 0; k < 16; k++) {
+                    const bool hit = cmp_bits(v[k], c.c, c.cf, true);
+                    cnt += hit;
+                    sum += hit ? v[k] : 0;
+                }
+            }
+        } else if (bi.kind == kItRest) {
+            for (uint64_t r = bi.start + lane; r < bi.start + bi.count; r += 32) {
+                const uint64_t v = __ldg(c.rest + (r - c.n_compr));
+                const bool hit = cmp_bits(v, c.c, c.cf, r < c.sfrom);
+                cnt += hit;
+                sum += hit ? v : 0;
+            }
+        } else {  // rle_f runs, decompressed: rows before sfrom compare signed, the rest unsigned
+            const uint64_t *pairs = reinterpret_cast<const uint64_t *>(c.data);
+            uint64_t row = bi.seek;
+            for (uint64_t r0 = bi.start; r0 < bi.start + bi.count; r0 += 32) {
+                const uint64_t r = r0 + lane;
+                const bool in = r < bi.start + bi.count;
+                const uint64_t v = in ? __ldg(pairs + 2 * r) : 0, len = in ? __ldg(pairs + 2 * r + 1) : 0;
+                uint64_t incl = len;
+#pragma unroll
+                for (int d = 1; d < 32; d <<= 1) {
+                    const uint64_t o = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+                    if (int(lane) >= d) incl += o;
+                }
+                const uint64_t rs = row + incl - len;
+                const uint64_t nsig = c.sfrom > rs ? minu(c.sfrom - rs, len) : 0;
+                const uint64_t add =
+                    (cmp_bits(v, c.c, c.cf, true) ? nsig : 0) + (cmp_bits(v, c.c, c.cf, false) ? len - nsig : 0);
+                cnt += add;
+                sum += v * add;
+                row += __shfl_sync(0xFFFFFFFFu, incl, 31);
+            }
+        }
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) {
+            cnt += __shfl_xor_sync(0xFFFFFFFFu, cnt, d);
+            sum += __shfl_xor_sync(0xFFFFFFFFu, sum, d);
+        }
+        if (lane == 0) {
+            if (cnt) atomicAdd(out_cnt + bi.col, (unsigned long long)cnt);
+            if (sum) atomicAdd(out_sum + bi.col, (unsigned long long)sum);
+        }
+        __syncwarp();
+        consumed++;
+    }
+    // a failed wait leaves copies in flight: wait for them (bounded) before leaving
+    if (!ok)
+        for (unsigned t = consumed + 1; t < issued; t++) mbar_wait(bar + t % S, (t / S) & 1u);
+    if (!ok && lane == 0) atomicOr(err, kErrTimeout);
+    if (bad && lane == 0) atomicOr(err, kErrCorrupt);
+}
+
+__global__ void k_pick_seeks(const uint64_t *__restrict__ carry, uint64_t nb, uint64_t first_slot,
+                             uint64_t *__restrict__ seeks) {
+    const uint64_t n_it = (nb + kBItemBlocks - 1) / kBItemBlocks;
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n_it * 8;
+         i += uint64_t(gridDim.x) * blockDim.x)
+        seeks[(first_slot + i / 8) * 8 + i % 8] = carry[(i / 8) * kBItemBlocks * 8 + i % 8];
+}
+
+// bit width of every column's first block (the decoder its items take)
+__global__ void k_first_bw(const BCol *__restrict__ cols, uint64_t n, uint8_t *__restrict__ out) {
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
+        const BCol &c = cols[i];
+        out[i] = c.index && c.n_compr ? uint8_t(idx_bw(c.index[0])) : uint8_t(c.bw);
+    }
+}
+
+// run lengths summed per item of kBItemRuns runs
+__global__ void k_rle_item_rows(const uint64_t *__restrict__ pairs, uint64_t runs, uint64_t *__restrict__ out) {
+    const unsigned lane = threadIdx.x & 31u;
+    const uint64_t n_it = (runs + kBItemRuns - 1) / kBItemRuns;
+    for (uint64_t i = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) / 32; i < n_it;
+         i += uint64_t(gridDim.x) * blockDim.x / 32) {
+        uint64_t s = 0;
+        for (uint64_t r = i * kBItemRuns + lane; r < minu(runs, (i + 1) * kBItemRuns); r += 32) s += pairs[2 * r + 1];
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) s += __shfl_xor_sync(0xFFFFFFFFu, s, d);
+        if (lane == 0) out[i] = s;
+    }
+}
+
+}  // namespace
+}  // namespace ms
+
+using namespace ms;
+
+struct ms_batch {
+    ms_arena *arena;
+    uint64_t n_cols, n_items, plan_bytes;
+    BCol *d_cols;
+    BItem *d_items;
+    uint64_t *d_seeks;
+    unsigned long long *d_head;
+    ms_tuning cfg;  // warps, stages, stage_bytes (per warp), ctas_per_sm
+    cudaGraphExec_t graph;
+    uint64_t *g_cnt, *g_sum;  // outputs the graph was captured for
+};
+
+namespace {
+
+size_t batch_shm(const ms_tuning &t) {
+    return size_t(t.warps) * (bwarp_meta_bytes(t.stages) + size_t(t.stages) * t.stage_bytes);
+}
+
+int batch_launch(ms_batch *b, uint64_t *d_cnt, uint64_t *d_sum, cudaStream_t st) {
+    MS_CUDA_TRY(cudaMemsetAsync(b->d_head, 0, 8, st));
+    if (!b->n_cols) return MS_OK;
+    MS_CUDA_TRY(cudaMemsetAsync(d_cnt, 0, 8 * b->n_cols, st));
+    MS_CUDA_TRY(cudaMemsetAsync(d_sum, 0, 8 * b->n_cols, st));
+    if (!b->n_items) return MS_OK;
+    const unsigned S = b->cfg.stages, SB = b->cfg.stage_bytes;
+    const size_t shm = batch_shm(b->cfg);
+    const unsigned grid = unsigned(sm_count()) * b->cfg.ctas_per_sm;
+#define MS_B(Wn)                                                                                                \
+    case Wn:                                                                                                    \
+        k_batch<Wn><<<grid, 32 * Wn, shm, st>>>(b->d_cols, b->d_items, b->n_items, b->d_seeks, S, SB, b->d_head, \
+                                                (unsigned long long *)d_cnt, (unsigned long long *)d_sum,        \
+                                                b->arena->d_err);                                               \
+        break;
+    switch (b->cfg.warps) {
+        MS_B(4) MS_B(8) MS_B(12) MS_B(16)
+    default: return ms_fail(MS_ERR_INVALID, "batch: warps must be 4, 8, 12 or 16");
+    }
+#undef MS_B
+    MS_CUDA_TRY(cudaGetLastError());
+    return MS_OK;
+}
+
+int batch_set_attr(const ms_tuning &t) {
+    const size_t shm = batch_shm(t);
+    int dev = 0, maxb = 0, maxsm = 0;
+    MS_CUDA_TRY(cudaGetDevice(&dev));
+    MS_CUDA_TRY(cudaDeviceGetAttribute(&maxb, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    MS_CUDA_TRY(cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+    if (shm > size_t(maxb) || (shm + 1024) * t.ctas_per_sm > size_t(maxsm))
+        return ms_fail(MS_ERR_INVALID, "batch: warps x stages x stage_bytes exceed shared memory");
+#define MS_B(Wn)                                                                                               \
+    case Wn:                                                                                                   \
+        MS_CUDA_TRY(cudaFuncSetAttribute(k_batch<Wn>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm))); \
+        break;
+    switch (t.warps) {
+        MS_B(4) MS_B(8) MS_B(12) MS_B(16)
+    default: return ms_fail(MS_ERR_INVALID, "batch: warps must be 4, 8, 12 or 16");
+    }
+#undef MS_B
+    return MS_OK;
+}
+
+int batch_fail(ms_batch *b, int rc) {
+    delete b;
+    return rc;
+}
+
+}  // namespace
+
+extern "C" int ms_gpu_batch_create(const ms_col *cols, const uint64_t *consts, uint64_t n_cols, int cmp, ms_arena *a,
+                                   ms_batch **out, void *stream) {
+    if (!out || !a || (n_cols && (!cols || !consts))) return ms_fail(MS_ERR_INVALID, "batch_create: null argument");
+    if (cmp < MS_CMP_EQ || cmp > MS_CMP_GE) return ms_fail(MS_ERR_INVALID, "batch_create: comparison");
+    *out = nullptr;
+    cudaStream_t st = (cudaStream_t)stream;
+    std::vector<BCol> hc(n_cols);
+    std::vector<BItem> hi;
+    std::vector<uint64_t> rle_cols, delta_cols, first_item(n_cols, 0);
+    uint64_t n_seek = 0;
+    for (uint64_t i = 0; i < n_cols; i++) {
+        const ms_col &c = cols[i];
+        int rc = check_col(&c, false);
+        if (rc) return rc;
+        BCol b{};
+        b.c = consts[i];
+        b.pred = make_pred(cmp, consts[i]);
+        b.cf = cmp_flags(cmp);
+        b.n = c.count_values;
+        if (c.format == MS_FMT_RLE) {
+            b.data = (const uint8_t *)c.data;
+            b.sfrom = c.count_values - c.count_values % kStep;  // as the decompressed column
+            const uint64_t runs = c.size_used_byte / 16;
+            first_item[i] = hi.size();
+            for (uint64_t r = 0; r < runs; r += kBItemRuns)
+                hi.push_back(BItem{uint32_t(i), kItRle, r, uint32_t(minu(kBItemRuns, runs - r)), 0, 0});
+            rle_cols.push_back(i);
+            hc[i] = b;
+            continue;
+        }
+        ColView v;
+        const uint64_t mark = a->used;
+        const bool had_index = c.format == MS_FMT_STATIC_VBP || c.format == MS_FMT_UNCOMPR ||
+                               (c.index && c.n_index >= (c.count_values - count_rest(c)) / kBlock &&
+                                (c.format != MS_FMT_FOR_DVBP || c.index_aux));
+        rc = prepare_view(&c, a, st, &v);  // builds a missing block index in the arena (kept)
+        if (rc) return rc;
+        if (c.format == MS_FMT_DELTA_DVBP && had_index) a->used = mark;  // delta carries: recomputed below
+        b.data = v.data;
+        b.index = v.index;
+        b.aux = v.aux;
+        b.rest = v.rest;
+        b.n_compr = v.n_compr;
+        b.sfrom = v.sfrom;
+        b.bw = v.bw;
+        const uint32_t kind = c.format == MS_FMT_FOR_DVBP ? kItFor : c.format == MS_FMT_DELTA_DVBP ? kItDelta : kItVbp;
+        const uint64_t nb = v.nb();
+        for (uint64_t s = 0; s < nb; s += kBItemBlocks)
+            hi.push_back(BItem{uint32_t(i), kind, s, uint32_t(minu(kBItemBlocks, nb - s)), 0,
+                               kind == kItDelta ? n_seek + s / kBItemBlocks : 0});
+        if (kind == kItDelta && nb) {
+            delta_cols.push_back(i);
+            first_item[i] = n_seek;  // its first seek slot
+            n_seek += (nb + kBItemBlocks - 1) / kBItemBlocks;
+        }
+        for (uint64_t r = v.n_compr; r < v.n; r += kBItemRest)
+            hi.push_back(BItem{uint32_t(i), kItRest, r, uint32_t(minu(kBItemRest, v.n - r)), 0, 0});
+        hc[i] = b;
+    }
+    ms_batch *b = new ms_batch{};
+    b->arena = a;
+    b->n_cols = n_cols;
+    b->n_items = hi.size();
+    b->cfg = ms_tuning{1, 12, 2, 8192, 1, 16};
+    b->d_cols = arena_take_t<BCol>(a, n_cols + 1);
+    b->d_items = arena_take_t<BItem>(a, hi.size() + 1);
+    b->d_seeks = arena_take_t<uint64_t>(a, 8 * n_seek + 8);
+    b->d_head = arena_take_t<unsigned long long>(a, 1);
+    if (!b->d_cols || !b->d_items || !b->d_seeks || !b->d_head)
+        return batch_fail(b, ms_fail(MS_ERR_NOMEM, "arena exhausted (batch plan)"));
+    b->plan_bytes = sizeof(BCol) * n_cols + sizeof(BItem) * hi.size() + 64 * n_seek;
+    // delta_f seeks: the carry into each item's first block
+    for (uint64_t i : delta_cols) {
+        const uint64_t mark = a->used;
+        ColView v;
+        int rc = prepare_view(&cols[i], a, st, &v);
+        if (rc) return batch_fail(b, rc);
+        k_pick_seeks<<<64, 256, 0, st>>>(v.carry, v.nb(), first_item[i], b->d_seeks);
+        MS_CUDA_TRY(cudaGetLastError());
+        MS_CUDA_TRY(cudaStreamSynchronize(st));
+        a->used = mark;
+    }
+    // rle_f: the first row of every item
+    for (uint64_t i : rle_cols) {
+        const uint64_t runs = cols[i].size_used_byte / 16;
+        const uint64_t n_it = (runs + kBItemRuns - 1) / kBItemRuns;
+        if (!n_it) continue;
+        const uint64_t mark = a->used;
+        uint64_t *tot = arena_take_t<uint64_t>(a, n_it);
+        if (!tot) return batch_fail(b, ms_fail(MS_ERR_NOMEM, "arena exhausted (batch plan)"));
+        k_rle_item_rows<<<64, 256, 0, st>>>((const uint64_t *)cols[i].data, runs, tot);
+        MS_CUDA_TRY(cudaGetLastError());
+        std::vector<uint64_t> h(n_it);
+        MS_CUDA_TRY(cudaMemcpyAsync(h.data(), tot, 8 * n_it, cudaMemcpyDeviceToHost, st));
+        MS_CUDA_TRY(cudaStreamSynchronize(st));
+        a->used = mark;
+        uint64_t row = 0;
+        for (uint64_t k = 0; k < n_it; k++) {
+            hi[first_item[i] + k].seek = row;
+            row += h[k];
+        }
+    }
+    if (n_cols) MS_CUDA_TRY(cudaMemcpyAsync(b->d_cols, hc.data(), sizeof(BCol) * n_cols, cudaMemcpyHostToDevice, st));
+    // Queue order: items that take the same decoder (kind, bit width) run
+    // together, so the warps of an SM share their instructions; the items of
+    // a column keep their order.
+    if (n_cols) {
+        const uint64_t mark = a->used;
+        uint8_t *d_bw = arena_take_t<uint8_t>(a, n_cols);
+        if (!d_bw) return batch_fail(b, ms_fail(MS_ERR_NOMEM, "arena exhausted (batch plan)"));
+        k_first_bw<<<unsigned(minu((n_cols + 255) / 256, 1024)), 256, 0, st>>>(b->d_cols, n_cols, d_bw);
+        MS_CUDA_TRY(cudaGetLastError());
+        std::vector<uint8_t> fbw(n_cols);
+        MS_CUDA_TRY(cudaMemcpyAsync(fbw.data(), d_bw, n_cols, cudaMemcpyDeviceToHost, st));
+        MS_CUDA_TRY(cudaStreamSynchronize(st));
+        a->used = mark;
+        std::stable_sort(hi.begin(), hi.end(), [&](const BItem &x, const BItem &y) {
+            const uint32_t kx = (x.kind << 8) | (x.kind <= kItDelta ? fbw[x.col] : 0u);
+            const uint32_t ky = (y.kind << 8) | (y.kind <= kItDelta ? fbw[y.col] : 0u);
+            return kx < ky;
+        });
+    }
+    if (!hi.empty())
+        MS_CUDA_TRY(cudaMemcpyAsync(b->d_items, hi.data(), sizeof(BItem) * hi.size(), cudaMemcpyHostToDevice, st));
+    MS_CUDA_TRY(cudaStreamSynchronize(st));
+    int rc = read_err(a, st);
+    if (rc) return batch_fail(b, rc);
+    rc = batch_set_attr(b->cfg);
+    if (rc) return batch_fail(b, rc);
+    *out = b;
+    return MS_OK;
+}
+
+extern "C" int ms_gpu_batch_set_config(ms_batch *b, const ms_tuning *t) {
+    if (!b || !t) return ms_fail(MS_ERR_INVALID, "batch_set_config: null argument");
+    if (t->stages < 2 || t->stages > 8 || t->stage_bytes < 4096 || t->stage_bytes % 128 || t->ctas_per_sm < 1 ||
+        t->ctas_per_sm > 4)
+        return ms_fail(MS_ERR_INVALID,
+                       "batch_set_config: stages 2..8, stage_bytes >= 4096 (multiple of 128), ctas_per_sm 1..4");
+    int rc = batch_set_attr(*t);
+    if (rc) return rc;
+    b->cfg = *t;
+    if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    return MS_OK;
+}
+
+extern "C" int ms_gpu_batch_get_config(const ms_batch *b, ms_tuning *t) {
+    if (!b || !t) return ms_fail(MS_ERR_INVALID, "batch_get_config: null argument");
+    *t = b->cfg;
+    return MS_OK;
+}
+
+extern "C" int ms_gpu_batch_run(ms_batch *b, uint64_t *d_counts, uint64_t *d_sums, void *stream) {
+    if (!b || (b->n_cols && (!d_counts || !d_sums))) return ms_fail(MS_ERR_INVALID, "batch_run: null argument");
+    return batch_launch(b, d_counts, d_sums, (cudaStream_t)stream);
+}
+
+extern "C" int ms_gpu_batch_run_graph(ms_batch *b, uint64_t *d_counts, uint64_t *d_sums, void *stream) {
+    if (!b || (b->n_cols && (!d_counts || !d_sums))) return ms_fail(MS_ERR_INVALID, "batch_run_graph: null argument");
+    if (b->graph && (b->g_cnt != d_counts || b->g_sum != d_sums)) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    if (!b->graph) {
+        cudaStream_t cs;
+        MS_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+        int rc = e == cudaSuccess ? batch_launch(b, d_counts, d_sums, cs) : MS_OK;
+        const cudaError_t e2 = e == cudaSuccess ? cudaStreamEndCapture(cs, &g) : cudaSuccess;
+        cudaStreamDestroy(cs);
+        MS_CUDA_TRY(e);
+        if (rc) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        MS_CUDA_TRY(e2);
+        e = cudaGraphInstantiate(&b->graph, g, 0);
+        cudaGraphDestroy(g);
+        MS_CUDA_TRY(e);
+        b->g_cnt = d_counts;
+        b->g_sum = d_sums;
+    }
+    MS_CUDA_TRY(cudaGraphLaunch(b->graph, (cudaStream_t)stream));
+    return MS_OK;
+}
+
+extern "C" int ms_gpu_batch_info(const ms_batch *b, uint64_t *n_items, uint64_t *plan_bytes) {
+    if (!b) return ms_fail(MS_ERR_INVALID, "batch_info: null");
+    if (n_items) *n_items = b->n_items;
+    if (plan_bytes) *plan_bytes = b->plan_bytes;
+    return MS_OK;
+}
+
+extern "C" void ms_gpu_batch_destroy(ms_batch *b) {
+    if (!b) return;
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    delete b;
+}

@@ -263,3 +263,72 @@ __device__ __forceinline__ uint64_t sum32_block_rt(unsigned bw, const uint64_t *
 }
 
 }  // namespace ms
+
+namespace ms {
+
+// Select and sum over the same plain vbp block, decoded once: cnt gets the
+// number of rows of thread (l, q) that pass, the return value their sum.
+template <unsigned BW>
+__device__ __forceinline__ uint64_t self_sum_block(const uint64_t *blk, unsigned l, unsigned q, const Pred &p,
+                                                   unsigned &cnt) {
+    unsigned m = 0;
+    if (BW <= 32) {
+        uint32_t v[16];
+        vbp_decode16_u32<(BW <= 32 ? BW : 32)>(blk, l, q, v);
+        if (p.is_eq) {
+            const bool in = p.val < (uint64_t(1) << 32);
+            const uint32_t c = uint32_t(p.val);
+#pragma unroll
+            for (int k = 0; k < 16; k++) m |= unsigned(in && v[k] == c) << k;
+        } else {
+            const bool big = p.T > 0xFFFFFFFFull;
+            const uint32_t T = uint32_t(p.T);
+#pragma unroll
+            for (int k = 0; k < 16; k++) m |= unsigned(big || v[k] < T) << k;
+            if (p.flip) m ^= 0xFFFFu;
+        }
+        cnt = __popc(m);
+        if (BW <= 27) {
+            uint32_t s = 0;
+#pragma unroll
+            for (int k = 0; k < 16; k++) s += ((m >> k) & 1u) ? v[k] : 0u;
+            return s;
+        }
+        uint64_t s = 0;
+#pragma unroll
+        for (int k = 0; k < 16; k++) s += ((m >> k) & 1u) ? v[k] : 0u;
+        return s;
+    } else {
+        uint64_t v[16];
+        vbp_decode16<BW, true>(blk, l, q, v);
+        if (BW == 64) {
+#pragma unroll
+            for (int k = 0; k < 16; k++) m |= unsigned(cmp_eval(p.cmp, v[k], p.val, true)) << k;
+        } else if (p.is_eq) {
+#pragma unroll
+            for (int k = 0; k < 16; k++) m |= unsigned(v[k] == p.val) << k;
+        } else {
+#pragma unroll
+            for (int k = 0; k < 16; k++) m |= unsigned(v[k] < p.T) << k;
+            if (p.flip) m ^= 0xFFFFu;
+        }
+        cnt = __popc(m);
+        uint64_t s = 0;
+#pragma unroll
+        for (int k = 0; k < 16; k++) s += ((m >> k) & 1u) ? v[k] : 0;
+        return s;
+    }
+}
+
+__device__ __forceinline__ uint64_t self_sum_block_rt(unsigned bw, const uint64_t *blk, unsigned l, unsigned q,
+                                                      const Pred &p, unsigned &cnt, bool &bad) {
+    switch (bw) {
+#define MS_X(B) \
+    case B: return self_sum_block<B>(blk, l, q, p, cnt);
+        MS_BW_CASES(MS_X)
+#undef MS_X
+    default: bad = true; cnt = 0; return 0;
+    }
+}
+
+}  // namespace ms

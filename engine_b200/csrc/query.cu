@@ -10,11 +10,11 @@
 // probes fk against the build side's bitmap, and for the surviving rows
 // decodes gkey and measure and folds (key, row, measure) into a per-CTA
 // shared-memory group table (warp-aggregated for skewed keys), flushed to a
-// global table at the end.  Each key keeps the smallest (row, rank of the row
-// among P in its block) pair, so after a scan of the per-block hit counts the
-// group's extent -- its first position in P, which is what the reference's
-// group operator returns -- is exact, and ordering groups by first row gives
-// the reference's group ids.  The result equals the operator-at-a-time
+// global table at the end.  Each key keeps its smallest row; after a scan of
+// the per-block hit counts, the group's extent -- the position of that row in
+// P, which is what the reference's group operator returns -- is the hits
+// before its block plus its rank within the block, and ordering groups by
+// first row gives the reference's group ids.  The result equals the operator-at-a-time
 // pipeline's bit for bit; no intermediate touches HBM.
 #include <algorithm>
 #include <vector>
@@ -40,7 +40,7 @@ __device__ __forceinline__ uint64_t qhash(uint64_t k) {
 
 struct GTable {  // global group table (open addressing)
     unsigned long long *keys;
-    unsigned long long *first;  // (row << 9) | rank of the row among the block's hits
+    unsigned long long *first;  // smallest row of the group
     unsigned long long *sums;
     uint64_t mask;
 };
@@ -92,8 +92,6 @@ __global__ void __launch_bounds__(256) k_query3(ColView filt, ColView fk, ColVie
         const unsigned total = __reduce_add_sync(0xFFFFFFFFu, __popc(m));
         if (lane == 0) blk_hits[b] = total;
         if (total == 0) continue;
-        unsigned rank[16];
-        block_ranks(m, l, q, rank);
         uint64_t g[16], w[16];
         unsigned vg, vm;
         ok &= decode_block(gkey, b, l, q, g, vg);
@@ -103,7 +101,7 @@ __global__ void __launch_bounds__(256) k_query3(ColView filt, ColView fk, ColVie
         for (int k = 0; k < 16; k++) {
             const bool hit = (m >> k) & 1u;
             const uint64_t key = g[k];
-            const uint64_t first = ((row0 + (16u * q + k) * 8u + l) << 9) | rank[k];
+            const uint64_t first = row0 + (16u * q + k) * 8u + l;
             // lanes with the same key combine first: one table update per key
             const unsigned hm = __ballot_sync(0xFFFFFFFFu, hit);
             if (!hit) continue;
@@ -354,8 +352,7 @@ __global__ void __launch_bounds__(32 * (W + 1), 1)
                             if (had[i] && !(inr[i] && ((word[i] >> bit[i]) & 1u))) m &= ~(1u << kk[i]);
                     }
                 }
-                unsigned rank[16];
-                const unsigned total = block_ranks(m, l, q, rank);
+                const unsigned total = __reduce_add_sync(0xFFFFFFFFu, __popc(m));
                 if (lane == 0) blk_hits[blk] = total;
                 if (total == 0) continue;
                 const uint64_t *gb = reinterpret_cast<const uint64_t *>(ring + o[2 * kQTile + j]);
@@ -373,12 +370,9 @@ __global__ void __launch_bounds__(32 * (W + 1), 1)
                     const unsigned hm = __ballot_sync(0xFFFFFFFFu, hit);
                     if (!hit) continue;
                     const unsigned k = __ffs(r) - 1;
-                    unsigned rk = 0;
-#pragma unroll
-                    for (unsigned kk = 0; kk < 16; kk++) rk = kk == k ? rank[kk] : rk;
                     const uint64_t key = vbp_extract(gb, gbw, l, 16u * q + k) + gref;
                     const uint64_t val = vbp_extract(mb, mbw, l, 16u * q + k) + mref;
-                    const uint64_t first = ((row0 + (16u * q + k) * 8u + l) << 9) | rk;
+                    const uint64_t first = row0 + (16u * q + k) * 8u + l;
                     const unsigned peers = __match_any_sync(hm, key);
                     uint64_t sm = val, f = first;
                     for (unsigned rest = peers; rest;) {
@@ -461,21 +455,51 @@ __global__ void k_minmax_q(ColView c, unsigned long long *mn, unsigned long long
     atomicMax(mx, (unsigned long long)hi);
 }
 
-// extent of every group (hits in earlier blocks + rank within its block),
-// compacted to dense arrays in slot-arrival order
-__global__ void k_q3_extents(GTable gt, const uint64_t *__restrict__ blk_off, unsigned long long *__restrict__ cnt,
-                             uint64_t *__restrict__ o_key, uint64_t *__restrict__ o_ext, uint64_t *__restrict__ o_sum,
-                             uint64_t *__restrict__ o_row) {
-    for (uint64_t h = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; h <= gt.mask; h += uint64_t(gridDim.x) * blockDim.x) {
-        if (gt.keys[h] == kQEmpty) continue;
-        const uint64_t f = gt.first[h];
-        const uint64_t r = f >> 9;
-        const unsigned long long i = atomicAdd(cnt, 1ull);
-        o_key[i] = gt.keys[h];
-        o_ext[i] = blk_off[r / kBlock] + (f & 511u);
-        o_sum[i] = gt.sums[h];
-        o_row[i] = r;
+// Extent of every group: its first row's position in P, i.e. the hits in
+// earlier blocks (scan of the per-block counts) plus the row's rank among the
+// hits of its own block, which one warp per group recomputes by decoding that
+// block of the filter and the foreign key again.  Results are compacted to
+// dense arrays in arrival order.
+__global__ void __launch_bounds__(256) k_q3_extents(GTable gt, ColView filt, ColView fk, int cmp, uint64_t c,
+                                                   const uint32_t *__restrict__ bits, uint64_t lo, uint64_t span,
+                                                   const uint64_t *__restrict__ blk_off,
+                                                   unsigned long long *__restrict__ cnt, uint64_t *__restrict__ o_key,
+                                                   uint64_t *__restrict__ o_ext, uint64_t *__restrict__ o_sum,
+                                                   uint64_t *__restrict__ o_row, unsigned *err) {
+    const unsigned lane = threadIdx.x & 31u, l = lane & 7u, q = lane >> 3;
+    bool ok = true;
+    for (uint64_t h = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) / 32; h <= gt.mask;
+         h += uint64_t(gridDim.x) * blockDim.x / 32) {
+        const uint64_t key = gt.keys[h];
+        if (key == kQEmpty) continue;
+        const uint64_t row = gt.first[h];
+        const uint64_t b = row / kBlock;
+        uint64_t v[16];
+        unsigned valid;
+        ok &= decode_block(filt, b, l, q, v, valid);
+        unsigned m = select_mask(filt, b, l, q, v, valid, cmp, c);
+        ok &= decode_block(fk, b, l, q, v, valid);
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+            const uint64_t d = v[k] - lo;
+            if (!(v[k] >= lo && d < span && ((bits[d >> 5] >> (d & 31u)) & 1u))) m &= ~(1u << k);
+        }
+        unsigned rank[16];
+        block_ranks(m, l, q, rank);
+        const unsigned s = unsigned(row % kBlock) / 8u;  // slot of the row within its lane
+        unsigned rk = 0;
+#pragma unroll
+        for (unsigned k = 0; k < 16; k++) rk = (16u * q + k == s) ? rank[k] : rk;
+        rk = __shfl_sync(0xFFFFFFFFu, rk, int((s / 16u) * 8u + unsigned(row % 8)));
+        if (lane == 0) {
+            const unsigned long long i = atomicAdd(cnt, 1ull);
+            o_key[i] = key;
+            o_ext[i] = blk_off[b] + rk;
+            o_sum[i] = gt.sums[h];
+            o_row[i] = row;
+        }
     }
+    if (!ok) atomicOr(err, kErrCorrupt);
 }
 
 bool random_access(const ColView &v) { return plain(v) || v.fmt == MS_FMT_FOR_DVBP; }
@@ -625,8 +649,9 @@ extern "C" int ms_gpu_query3(const ms_col *filter, int cmp, uint64_t c, const ms
                 MS_CUDA_TRY(cudaGetLastError());
             }
             MS_CUDA_TRY((scan_exclusive<uint32_t, 1>(hits, nbt, boff, tot, scr, st)));
-            k_q3_extents<<<unsigned(minu(slots / 256, 1024)), 256, 0, st>>>(gt, boff, cnt, out, out + slots,
-                                                                          out + 2 * slots, out + 3 * slots);
+            k_q3_extents<<<unsigned(minu(slots / 8, 4096)), 256, 0, st>>>(
+                gt, fv, kv, cmp, c, bits, lo, span, boff, cnt, out, out + slots, out + 2 * slots, out + 3 * slots,
+                a->d_err);
             MS_CUDA_TRY(cudaGetLastError());
         }
         unsigned herr = 0;

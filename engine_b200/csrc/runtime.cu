@@ -347,6 +347,35 @@ int ms::build_index_device(const ms_col *c, uint64_t *index, uint64_t *aux, unsi
     return MS_OK;
 }
 
+// Copy a column into storage of exactly its used size (the producing
+// operators allocate the format's worst case, get_size_max_byte_any_len),
+// block index included.
+extern "C" int ms_gpu_col_compact(const ms_col *in, ms_col *out, ms_arena *a, void *stream) {
+    using namespace ms;
+    if (!in || !out || !a) return ms_fail(MS_ERR_INVALID, "col_compact: null");
+    int rc = check_col(in, false);
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    const uint64_t bytes = in->size_used_byte;
+    const bool has_index = in->index && in->n_index, has_aux = in->index_aux && in->n_index;
+    uint8_t *data = arena_take_t<uint8_t>(a, bytes + 64);
+    uint64_t *index = has_index ? arena_take_t<uint64_t>(a, in->n_index + 1) : nullptr;
+    uint64_t *aux = has_aux ? arena_take_t<uint64_t>(a, in->n_index / 2 + 1) : nullptr;
+    if (!data || (has_index && !index) || (has_aux && !aux)) return ms_fail(MS_ERR_NOMEM, "arena exhausted (col_compact)");
+    if (bytes) MS_CUDA_TRY(cudaMemcpyAsync(data, in->data, bytes, cudaMemcpyDeviceToDevice, st));
+    if (index) MS_CUDA_TRY(cudaMemcpyAsync(index, in->index, 8 * in->n_index, cudaMemcpyDeviceToDevice, st));
+    if (aux && in->n_index / 2)
+        MS_CUDA_TRY(cudaMemcpyAsync(aux, in->index_aux, 8 * (in->n_index / 2), cudaMemcpyDeviceToDevice, st));
+    ms_col c = *in;
+    c.data = data;
+    c.size_alloc_byte = bytes + 64;
+    c.index = index;
+    c.index_aux = aux;
+    if (!index) c.n_index = 0;
+    *out = c;
+    return MS_OK;
+}
+
 extern "C" int ms_gpu_build_index(ms_col *c, ms_arena *a, void *stream) {
     using namespace ms;
     if (!c || !a) return ms_fail(MS_ERR_INVALID, "build_index: null");

@@ -139,6 +139,11 @@ int ms_gpu_morph(const ms_col *src, int dst_format, unsigned dst_bw, ms_col *out
                  ms_arena *arena, void *stream);
 /* Build ms_col.index for a device column (device-side page walk). */
 int ms_gpu_build_index(ms_col *col, ms_arena *arena, void *stream);
+/* Copy a column (data and block index) into storage of exactly its used
+ * size in `arena`: operators allocate the format's worst case
+ * (get_size_max_byte_any_len, format.h:114-153), so a column that is kept
+ * can be compacted after it is produced.  Asynchronous. */
+int ms_gpu_col_compact(const ms_col *in, ms_col *out, ms_arena *arena, void *stream);
 
 /* ---- operators (include/core/operators/interfaces/) ----------------------- */
 /* agg_sum<ve,F>(col) (agg_sum.h:56-65; agg_sum_compr.h:78-153): the uint64
@@ -232,6 +237,30 @@ int ms_gpu_query3(const ms_col *filter, int cmp, uint64_t c, const ms_col *fk, c
  * does not fit shared memory with the 48 KiB group table. */
 int ms_gpu_set_query_tuning(const ms_tuning *t);
 int ms_gpu_get_query_tuning(ms_tuning *t);
+
+/* ---- batched persistent execution (no counterpart as one call in the
+ * reference: for every column i it runs the chain morph<uncompr_f> ->
+ * select<cmp>(c_i) -> agg_sum of the selected values, select_compr.h:100-260
+ * with project_compr.h and agg_sum_compr.h, over many columns in one
+ * persistent launch off a device work queue) --------------------------------
+ * ms_gpu_batch_create builds the plan (work items, per-item seek values for
+ * delta_f and rle_f) in the arena; the columns and the arena must outlive it.
+ * ms_gpu_batch_run launches it (memsets and one kernel, no host
+ * synchronisation): d_counts[i] / d_sums[i] receive column i's hit count and
+ * the sum of its selected values (mod 2^64).  ms_gpu_batch_run_graph does
+ * the same through a CUDA graph captured on first use for these output
+ * buffers.  Kernel errors are reported by ms_gpu_arena_check. */
+typedef struct ms_batch ms_batch;
+int ms_gpu_batch_create(const ms_col *cols, const uint64_t *consts, uint64_t n_cols, int cmp, ms_arena *arena,
+                        ms_batch **out, void *stream);
+/* warps per CTA (4, 8, 12, 16), stages and stage_bytes of each warp's ring,
+ * ctas_per_sm; other fields ignored */
+int ms_gpu_batch_set_config(ms_batch *b, const ms_tuning *t);
+int ms_gpu_batch_get_config(const ms_batch *b, ms_tuning *t);
+int ms_gpu_batch_run(ms_batch *b, uint64_t *d_counts, uint64_t *d_sums, void *stream);
+int ms_gpu_batch_run_graph(ms_batch *b, uint64_t *d_counts, uint64_t *d_sums, void *stream);
+int ms_gpu_batch_info(const ms_batch *b, uint64_t *n_items, uint64_t *plan_bytes);
+void ms_gpu_batch_destroy(ms_batch *b);
 
 /* ---- per-block format selection and the learned selector ------------------
  * Blocks of ms_gpu_sel_block_values() = 2048 values; five candidates per block

@@ -123,3 +123,18 @@ def test_device_generators_match_oracle(ms, arena, orc):
     for gen, expect in checks:
         ms._check(gen(), "gen")
         assert np.array_equal(ms._memcpy_d2h(out, 8 * n).view(np.uint64), expect)
+
+
+@pytest.mark.parametrize("fmt", [O.STATIC_VBP, O.DYNAMIC_VBP, O.DELTA_DVBP, O.FOR_DVBP, O.RLE])
+def test_compact_keeps_column(ms, arena, orc, fmt):
+    """A compacted column has the same bytes, metadata and values, in
+    storage of its used size."""
+    v = _values(orc, fmt, 9, 40_000 + 3, seed=4)
+    c = ms.morph(ms.Column.from_numpy(v, arena), _fmt(ms, fmt, 9))
+    k = c.compact()
+    assert k.meta() == c.meta()
+    assert k.desc.size_alloc_byte == c.get_size_used_byte() + 64
+    assert np.array_equal(k.raw_bytes(), c.raw_bytes())
+    assert np.array_equal(k.to_numpy(), v)
+    if fmt != O.RLE:
+        assert ms.select_project_sum(k, ms.less, 1000, k) == ms.select_project_sum(c, ms.less, 1000, c)
