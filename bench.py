@@ -315,6 +315,10 @@ def run_gpu(args):
         from engine_b200 import star_query
         line["star_query"] = star_query.run(args.log2_rows, 5)
         ok = ok and line["star_query"]["bit_exact"]
+    if not args.no_batch and world == 1:
+        from engine_b200 import batch_bench
+        line["batched"] = batch_bench.run(4096, 10, per_column_steps=1)
+        ok = ok and line["batched"]["bit_exact"]
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
             line["cpu_baseline"] = cpu_baseline(1)
@@ -534,6 +538,7 @@ def main():
     ap.add_argument("--sel-log2-eval", type=int, default=30, help="evaluation column values = 2^N")
     ap.add_argument("--sel-steps", type=int, default=2000, help="Adam steps")
     ap.add_argument("--no-star", action="store_true", help="skip the fused star-query leg")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched many-column leg")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -479,7 +479,7 @@ def query3(filter_col: Column, cmp: int, c: int, fk: Column, l: Column, gkey: Co
     return keys[:k], ext[:k], sums[:k], int(npos.value)
 
 
-def set_query_tuning(staged: int = 1, warps: int = 16, stages: int = 4, stage_bytes: int = 40960) -> None:
+def set_query_tuning(staged: int = 1, warps: int = 16, stages: int = 3, stage_bytes: int = 57344) -> None:
     """Launch configuration of query3's staged kernel."""
     t = MsTuning(staged=staged, warps=warps, stages=stages, stage_bytes=stage_bytes, ctas_per_sm=1,
                  values_per_thread=16)

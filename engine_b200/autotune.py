@@ -23,7 +23,7 @@ CACHE = os.path.join(HERE, "tuning.json")
 
 CANDIDATES = [dict(staged=0, warps=8, stages=8, stage_bytes=24576, ctas_per_sm=1, values_per_thread=16)] + [
     dict(staged=1, warps=w, stages=s, stage_bytes=b, ctas_per_sm=1, values_per_thread=v)
-    for v, w, s, b in itertools.product((16, 32), (12, 16, 24), (3, 4, 6), (24576, 32768, 49152, 65536))
+    for v, w, s, b in itertools.product((16, 32), (12, 16, 20, 24), (3, 4, 6), (24576, 32768, 49152, 65536))
     if s * b <= 200 * 1024
 ]
 

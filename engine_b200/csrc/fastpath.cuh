@@ -202,10 +202,51 @@ __device__ __forceinline__ void vbp_decode32_u32(const uint64_t *__restrict__ bl
     }
 }
 
+// Threshold test v < T for the 32 values of half h of lane l (BW <= 32,
+// T < 2^BW) without isolating the values: each field is shifted to the top
+// of a 32-bit word, where the bits below it (the next fields) are less than
+// 2^(32-BW), so  v < T  <=>  top < T * 2^(32-BW).  One shift and one compare
+// per value.
+template <unsigned BW>
+__device__ __forceinline__ unsigned vbp_lt32_top(const uint64_t *__restrict__ blk, unsigned l, unsigned h,
+                                                 uint32_t T) {
+    static_assert(BW <= 32, "32-bit fields");
+    constexpr unsigned NW = (32 * BW + 63) / 64 + 1;
+    constexpr unsigned NH = BW + 1;
+    const unsigned sbit = 32u * h * BW;
+    const unsigned w0 = sbit >> 6;
+    uint32_t hw[2 * NW];
+#pragma unroll
+    for (unsigned i = 0; i < NW; i++) {
+        const uint64_t w = (w0 + i < BW) ? blk[(w0 + i) * 8 + l] : 0;
+        hw[2 * i] = uint32_t(w);
+        hw[2 * i + 1] = uint32_t(w >> 32);
+    }
+    const unsigned o = (sbit >> 5) & 1u;
+    uint32_t n[NH];
+#pragma unroll
+    for (unsigned i = 0; i < NH; i++) {
+        if (BW % 2 == 0) n[i] = (i < 2 * NW) ? hw[i] : 0;
+        else n[i] = (i + 1 < 2 * NW) ? (o ? hw[i + 1] : hw[i]) : ((i < 2 * NW && !o) ? hw[i] : 0);
+    }
+    const uint32_t Tt = BW == 32 ? T : (T << (32u - BW));
+    unsigned m = 0;
+#pragma unroll
+    for (unsigned k = 0; k < 32; k++) {
+        const unsigned p = k * BW, wi = p >> 5, sh = p & 31u;
+        const uint32_t top = (sh + BW <= 32) ? (n[wi] << (32u - sh - BW)) : __funnelshift_r(n[wi], n[wi + 1], sh + BW - 32u);
+        m |= unsigned(top < Tt) << k;
+    }
+    return m;
+}
+
 template <unsigned BW>
 __device__ __forceinline__ unsigned mask32_block(const uint64_t *blk, unsigned l, unsigned h, const Pred &p) {
     unsigned m = 0;
-    if (BW <= 32) {
+    if (BW <= 32 && !p.is_eq && p.T < (uint64_t(1) << (BW <= 32 ? BW : 32))) {
+        m = vbp_lt32_top<(BW <= 32 ? BW : 32)>(blk, l, h, uint32_t(p.T));
+        if (p.flip) m = ~m;
+    } else if (BW <= 32) {
         uint32_t v[32];
         vbp_decode32_u32<(BW <= 32 ? BW : 32)>(blk, l, h, v);
         if (p.is_eq) {

@@ -505,7 +505,7 @@ __global__ void __launch_bounds__(256) k_q3_extents(GTable gt, ColView filt, Col
 bool random_access(const ColView &v) { return plain(v) || v.fmt == MS_FMT_FOR_DVBP; }
 
 // launch configuration of the staged kernel (consumer warps 8/16/24)
-ms_tuning g_q3 = {1, 16, 4, 40960, 1, 16};
+ms_tuning g_q3 = {1, 16, 3, 57344, 1, 16};
 
 template <int W>
 int launch_q3_tma_w(const ColView &fv, const ColView &kv, const ColView &gv, const ColView &mv, const StreamCol &s0,

@@ -27,8 +27,8 @@ ms_tuning ms::tuning() { return g_tuning; }
 extern "C" int ms_gpu_set_tuning(const ms_tuning *t) {
     if (!t) return ms_fail(MS_ERR_INVALID, "set_tuning: null");
     if (t->staged) {
-        if (t->warps != 4 && t->warps != 8 && t->warps != 12 && t->warps != 16 && t->warps != 24)
-            return ms_fail(MS_ERR_INVALID, "set_tuning: warps must be 4, 8, 12, 16 or 24");
+        if (t->warps != 4 && t->warps != 8 && t->warps != 12 && t->warps != 16 && t->warps != 20 && t->warps != 24)
+            return ms_fail(MS_ERR_INVALID, "set_tuning: warps must be 4, 8, 12, 16, 20 or 24");
         if (t->stages < 2 || t->stages > 32 || t->stage_bytes < 8320 || t->stage_bytes % 128 ||
             uint64_t(t->stages) * t->stage_bytes > 220 * 1024 || t->ctas_per_sm < 1 || t->ctas_per_sm > 4 ||
             (t->values_per_thread != 16 && t->values_per_thread != 32))

@@ -332,7 +332,7 @@ int launch_tma(const ColView &x, const ColView &y, int cmp, uint64_t val, const 
 
 // Fused select -> project -> agg_sum through the staged pipeline.  Columns
 // must be uncompr / static_vbp or carry a block index (dynamic_vbp, for_f)
-// or a prepared delta view.  warps: consumer warps per CTA (4, 8, 12, 16, 24).
+// or a prepared delta view.  warps: consumer warps per CTA (4, 8, 12, 16, 20, 24).
 int sps_tma(const ColView &x, const ColView &y, bool has_y, int cmp, uint64_t val, unsigned warps, unsigned stages,
             unsigned stage_bytes, unsigned ctas_per_sm, unsigned vpt, uint64_t *d_sum, uint64_t *d_cnt,
             unsigned *d_err, cudaStream_t st) {
@@ -344,9 +344,9 @@ int sps_tma(const ColView &x, const ColView &y, bool has_y, int cmp, uint64_t va
     if (warps == Wn)                                                                                      \
         return has_y ? launch_tma<Wn, true>(x, y, cmp, val, cfg, vpt, d_sum, d_cnt, d_err, grid, st)      \
                      : launch_tma<Wn, false>(x, x, cmp, val, cfg, vpt, d_sum, d_cnt, d_err, grid, st);
-    MS_L(4) MS_L(8) MS_L(12) MS_L(16) MS_L(24)
+    MS_L(4) MS_L(8) MS_L(12) MS_L(16) MS_L(20) MS_L(24)
 #undef MS_L
-    return ms_fail(MS_ERR_INVALID, "sps_tma: warps must be 4, 8, 12, 16 or 24");
+    return ms_fail(MS_ERR_INVALID, "sps_tma: warps must be 4, 8, 12, 16, 20 or 24");
 }
 
 }  // namespace ms

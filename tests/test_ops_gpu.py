@@ -132,6 +132,7 @@ def test_select_project_sum(ms, arena, orc, xcode, xbw, ycode, ybw, n):
     dict(staged=1, warps=24, stages=4, stage_bytes=49152, values_per_thread=16),
     dict(staged=1, warps=12, stages=6, stage_bytes=24576, values_per_thread=32),
     dict(staged=1, warps=24, stages=4, stage_bytes=49152, values_per_thread=32),
+    dict(staged=1, warps=20, stages=3, stage_bytes=65536, values_per_thread=32),
 ])
 @pytest.mark.parametrize("xcode,ycode", [(O.DYNAMIC_VBP, O.DYNAMIC_VBP), (O.STATIC_VBP, O.UNCOMPR),
                                          (O.FOR_DVBP, O.DELTA_DVBP)])
@@ -153,3 +154,28 @@ def test_select_project_sum_every_launch_config(ms, arena, orc, cfg, xcode, ycod
             assert (s, k) == orc.select_project_sum(cmp, c, x, y, sf), (cmp, c)
     finally:
         ms.set_tuning(**old)
+
+
+@pytest.mark.parametrize("bw", list(range(1, 33)))
+def test_threshold_path_every_width(ms, arena, orc, bw):
+    """The in-register threshold test of the 32-values-per-thread path at
+    every width up to 32 bits, with constants at the edges of the value
+    range (0, 1, half, 2^bw - 1, 2^bw) and every comparison."""
+    n = 4 * 1024 + 8 * 512 + 5
+    x = orc.uniform_bits(100 + bw, bw, n)
+    y = orc.uniform_bits(200 + bw, 20, n)
+    xc = ms.morph(ms.Column.from_numpy(x, arena), ms.static_vbp_f(bw))
+    xd = ms.morph(ms.Column.from_numpy(x, arena), ms.dynamic_vbp_f)
+    yc = ms.morph(ms.Column.from_numpy(y, arena), ms.dynamic_vbp_f)
+    old = ms.get_tuning()
+    try:
+        ms.set_tuning(**{**old, **dict(staged=1, warps=16, stages=3, stage_bytes=65536, values_per_thread=32)})
+        for c in sorted({0, 1, 1 << (bw - 1), (1 << bw) - 1, 1 << bw}):
+            for cmp in (O.CMP_LT, O.CMP_LE, O.CMP_GT, O.CMP_GE):
+                for col, code, cbw in ((xc, O.STATIC_VBP, bw), (xd, O.DYNAMIC_VBP, 0)):
+                    sf = orc.scalar_from(code, cbw, col.meta())
+                    assert ms.select_project_sum(col, cmp, c, yc) == orc.select_project_sum(cmp, c, x, y, sf), \
+                        (bw, c, cmp, code)
+    finally:
+        ms.set_tuning(**old)
+
