@@ -76,10 +76,51 @@ __device__ __forceinline__ void vbp_decode16_u32(const uint64_t *__restrict__ bl
     }
 }
 
+// v < T for the 16 values of quarter q of lane l (BW <= 32, T < 2^BW) on
+// top-aligned fields: the bits below a field shifted to the top of a 32-bit
+// word are less than 2^(32-BW), so  v < T  <=>  top < T * 2^(32-BW).
+template <unsigned BW>
+__device__ __forceinline__ unsigned vbp_lt16_top(const uint64_t *__restrict__ blk, unsigned l, unsigned q,
+                                                 uint32_t T) {
+    static_assert(BW <= 32, "32-bit fields");
+    constexpr unsigned NW = (16 * BW + 63) / 64 + 1;
+    constexpr unsigned NH = (16 * BW + 31) / 32 + 1;
+    const unsigned sbit = 16u * q * BW;
+    const unsigned w0 = sbit >> 6;
+    uint32_t h[2 * NW];
+#pragma unroll
+    for (unsigned i = 0; i < NW; i++) {
+        const uint64_t w = (w0 + i < BW) ? blk[(w0 + i) * 8 + l] : 0;
+        h[2 * i] = uint32_t(w);
+        h[2 * i + 1] = uint32_t(w >> 32);
+    }
+    const unsigned o = (sbit >> 5) & 1u;
+    const unsigned t = sbit & 31u;
+    uint32_t n[NH];
+#pragma unroll
+    for (unsigned i = 0; i < NH; i++) {
+        const uint32_t a = (i + 1 < 2 * NW) ? (o ? h[i + 1] : h[i]) : 0;
+        const uint32_t b = (i + 2 < 2 * NW) ? (o ? h[i + 2] : h[i + 1]) : ((i + 1 < 2 * NW && !o) ? h[i + 1] : 0);
+        n[i] = (BW % 2 == 0) ? a : __funnelshift_r(a, b, t);
+    }
+    const uint32_t Tt = BW == 32 ? T : (T << (32u - BW));
+    unsigned m = 0;
+#pragma unroll
+    for (unsigned k = 0; k < 16; k++) {
+        const unsigned p = k * BW, wi = p >> 5, sh = p & 31u;
+        const uint32_t top = (sh + BW <= 32) ? (n[wi] << (32u - sh - BW)) : __funnelshift_r(n[wi], n[wi + 1], sh + BW - 32u);
+        m |= unsigned(top < Tt) << k;
+    }
+    return m;
+}
+
 template <unsigned BW>
 __device__ __forceinline__ unsigned mask_block(const uint64_t *blk, unsigned l, unsigned q, const Pred &p) {
     unsigned m = 0;
-    if (BW <= 32) {
+    if (BW <= 32 && !p.is_eq && p.T < (uint64_t(1) << (BW <= 32 ? BW : 32))) {
+        m = vbp_lt16_top<(BW <= 32 ? BW : 32)>(blk, l, q, uint32_t(p.T));
+        if (p.flip) m ^= 0xFFFFu;
+    } else if (BW <= 32) {
         uint32_t v[16];
         vbp_decode16_u32<(BW <= 32 ? BW : 32)>(blk, l, q, v);
         if (p.is_eq) {
