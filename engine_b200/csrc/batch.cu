@@ -89,6 +89,110 @@ __device__ __forceinline__ bool cmp_bits(uint64_t v, uint64_t c, unsigned cf, bo
 
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
+// Threshold form of `base + d  cmp  c` (signed 64-bit, as the compressed
+// part compares) for d in [0, range), range <= 2^32: a Pred on d.  False when
+// base + [0, range) wraps or crosses the signed boundary -- then the order of
+// d is not the order of the values and the caller compares 64-bit values.
+__device__ __forceinline__ bool rel_pred(uint64_t base, uint64_t range, uint64_t c, int cmp, Pred &p) {
+    const uint64_t hi = base + (range - 1);
+    if (hi < base || ((int64_t)base < 0) != ((int64_t)hi < 0)) return false;
+    const int64_t cs = (int64_t)c, bs = (int64_t)base;
+    const uint64_t diff = uint64_t(cs) - uint64_t(bs);  // the true difference when cs >= bs
+    const uint64_t nlt = cs <= bs ? 0 : minu(diff, range);
+    const uint64_t nle = cs < bs ? 0 : (diff >= range ? range : diff + 1);
+    p.cmp = cmp;
+    p.val = c - base;
+    p.is_eq = cmp == MS_CMP_EQ;
+    p.T = (cmp == MS_CMP_LT || cmp == MS_CMP_GE) ? nlt : nle;
+    p.flip = cmp == MS_CMP_GT || cmp == MS_CMP_GE;
+    return true;
+}
+
+// A delta_f block of width BW <= 27 in 32-bit arithmetic: thread (l, q)
+// decodes its 16 deltas, forms their running sums P_k (< 2^31), and the
+// lane's values are base + P_k with base = carry + the sums of the lane's
+// earlier quarters.  The comparison becomes a threshold on P_k (rel_pred)
+// unless the thread's values cross the signed boundary; sums are cnt * base
+// + the sum of the selected P_k.  Returns the lane's last value (the carry of
+// the next block).
+template <unsigned BW>
+__device__ __forceinline__ uint64_t delta_block(const uint64_t *blk, unsigned l, unsigned q, uint64_t carry,
+                                                uint64_t c, int cmp, unsigned cf, uint64_t &cnt, uint64_t &sum) {
+    uint32_t P[16];
+    vbp_decode16_u32<BW>(blk, l, q, P);
+#pragma unroll
+    for (int k = 1; k < 16; k++) P[k] += P[k - 1];
+    const uint64_t tot = P[15];
+    const uint64_t up = __shfl_up_sync(0xFFFFFFFFu, tot, 8);
+    uint64_t pre = q >= 1 ? up : 0;
+    const uint64_t up2 = __shfl_up_sync(0xFFFFFFFFu, tot + pre, 16);
+    pre += q >= 2 ? up2 : 0;
+    const uint64_t base = carry + pre;
+    Pred pd;
+    unsigned m = 0;
+    if (rel_pred(base, uint64_t(P[15]) + 1, c, cmp, pd)) {
+        if (pd.is_eq) {
+            const bool in = pd.val < (uint64_t(1) << 32);
+#pragma unroll
+            for (int k = 0; k < 16; k++) m |= unsigned(in && P[k] == uint32_t(pd.val)) << k;
+        } else {
+            const bool big = pd.T > 0xFFFFFFFFull;
+#pragma unroll
+            for (int k = 0; k < 16; k++) m |= unsigned(big || P[k] < uint32_t(pd.T)) << k;
+            if (pd.flip) m ^= 0xFFFFu;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < 16; k++) m |= unsigned(cmp_bits(base + P[k], c, cf, true)) << k;
+    }
+    uint64_t s = 0;
+#pragma unroll
+    for (int k = 0; k < 16; k++) s += ((m >> k) & 1u) ? P[k] : 0u;
+    const unsigned n = __popc(m);
+    cnt += n;
+    sum += s + n * base;
+    return __shfl_sync(0xFFFFFFFFu, base + P[15], int(24 + l));
+}
+
+// Generic delta_f block (any width): 64-bit decode and running sums.
+__device__ __forceinline__ uint64_t delta_block_any(unsigned bw, const uint64_t *blk, unsigned l, unsigned q,
+                                                    uint64_t carry, uint64_t c, unsigned cf, uint64_t &cnt,
+                                                    uint64_t &sum, bool &bad) {
+    uint64_t v[16];
+    bad |= !vbp_decode16_rt<true>(bw, blk, l, q, v);
+#pragma unroll
+    for (int k = 1; k < 16; k++) v[k] += v[k - 1];
+    const uint64_t tot = v[15];
+    const uint64_t up = __shfl_up_sync(0xFFFFFFFFu, tot, 8);
+    uint64_t pre = q >= 1 ? up : 0;
+    const uint64_t up2 = __shfl_up_sync(0xFFFFFFFFu, tot + pre, 16);
+    pre += (q >= 2 ? up2 : 0) + carry;
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+        v[k] += pre;
+        const bool hit = cmp_bits(v[k], c, cf, true);
+        cnt += hit;
+        sum += hit ? v[k] : 0;
+    }
+    return __shfl_sync(0xFFFFFFFFu, v[15], int(24 + l));
+}
+
+#define MS_BW27(X)                                                                                      \
+    X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16) X(17) X(18) \
+    X(19) X(20) X(21) X(22) X(23) X(24) X(25) X(26) X(27)
+
+__device__ __forceinline__ uint64_t delta_block_rt(unsigned bw, const uint64_t *blk, unsigned l, unsigned q,
+                                                   uint64_t carry, uint64_t c, int cmp, unsigned cf, uint64_t &cnt,
+                                                   uint64_t &sum, bool &bad) {
+    switch (bw) {
+#define MS_X(B) \
+    case B: return delta_block<B>(blk, l, q, carry, c, cmp, cf, cnt, sum);
+        MS_BW27(MS_X)
+#undef MS_X
+    default: return delta_block_any(bw, blk, l, q, carry, c, cf, cnt, sum, bad);
+    }
+}
+
 __host__ __device__ inline unsigned bwarp_meta_bytes(unsigned S) {
     return (8u * S + unsigned(sizeof(BStage)) * S + 127u) / 128u * 128u;
 }
@@ -221,35 +325,36 @@ __global__ void __launch_bounds__(32 * W, 1)
                 sum += self_sum_block_rt(sd.bw[j], blk, l, q, c.pred, k, bad);
                 cnt += k;
             }
-        } else if (bi.kind == kItFor || bi.kind == kItDelta) {
-            if (bi.kind == kItDelta && sd.b0 == bi.start) carry = __ldg(seeks + bi.seek * 8 + l);
+        } else if (bi.kind == kItFor) {
             for (unsigned j = 0; j < sd.nblk; j++) {
-                uint64_t v[16];
-                bad |= !vbp_decode16_rt<true>(sd.bw[j], reinterpret_cast<const uint64_t *>(base + sd.off[j]), l, q, v);
-                if (bi.kind == kItFor) {
-                    const uint64_t ref = __ldg(c.aux + ((sd.b0 + j) >> 1));
-#pragma unroll
-                    for (int k = 0; k < 16; k++) v[k] += ref;
+                const uint64_t *blk = reinterpret_cast<const uint64_t *>(base + sd.off[j]);
+                const unsigned bw = sd.bw[j];
+                const uint64_t ref = __ldg(c.aux + ((sd.b0 + j) >> 1));
+                Pred pd;
+                if (bw <= 32 && rel_pred(ref, uint64_t(1) << bw, c.c, c.pred.cmp, pd)) {
+                    // values ref + d: select and sum on d in the bit-width switch
+                    unsigned k = 0;
+                    const uint64_t sd_ = self_sum_block_rt(bw, blk, l, q, pd, k, bad);
+                    cnt += k;
+                    sum += sd_ + uint64_t(k) * ref;
                 } else {
+                    uint64_t v[16];
+                    bad |= !vbp_decode16_rt<true>(bw, blk, l, q, v);
+                    // every row of the compressed part precedes the scalar remainder
 #pragma unroll
-                    for (int k = 1; k < 16; k++) v[k] += v[k - 1];
-                    const uint64_t tot = v[15];
-                    const uint64_t up = __shfl_up_sync(0xFFFFFFFFu, tot, 8);
-                    uint64_t pre = q >= 1 ? up : 0;
-                    const uint64_t up2 = __shfl_up_sync(0xFFFFFFFFu, tot + pre, 16);
-                    pre += (q >= 2 ? up2 : 0) + carry;
-#pragma unroll
-                    for (int k = 0; k < 16; k++) v[k] += pre;
-                    carry = __shfl_sync(0xFFFFFFFFu, v[15], int(24 + l));  // lane l's last value
-                }
-                // every row of the compressed part precedes the scalar remainder
-#pragma unroll
-                for (int k = 0; k < 16; k++) {
-                    const bool hit = cmp_bits(v[k], c.c, c.cf, true);
-                    cnt += hit;
-                    sum += hit ? v[k] : 0;
+                    for (int k = 0; k < 16; k++) {
+                        const uint64_t x = v[k] + ref;
+                        const bool hit = cmp_bits(x, c.c, c.cf, true);
+                        cnt += hit;
+                        sum += hit ? x : 0;
+                    }
                 }
             }
+        } else if (bi.kind == kItDelta) {
+            if (sd.b0 == bi.start) carry = __ldg(seeks + bi.seek * 8 + l);
+            for (unsigned j = 0; j < sd.nblk; j++)
+                carry = delta_block_rt(sd.bw[j], reinterpret_cast<const uint64_t *>(base + sd.off[j]), l, q, carry,
+                                       c.c, c.pred.cmp, c.cf, cnt, sum, bad);
         } else if (bi.kind == kItRest) {
             for (uint64_t r = bi.start + lane; r < bi.start + bi.count; r += 32) {
                 const uint64_t v = __ldg(c.rest + (r - c.n_compr));

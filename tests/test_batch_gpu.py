@@ -114,9 +114,18 @@ def test_batch_wide_values(ms, arena, orc):
             ms.morph(ms.Column.from_numpy(v40, arena), ms.dynamic_vbp_f)]
     vals = [v64, v64, v40, v40]
     consts = [1 << 62, 0, 1 << 41, 0]
-    cnt, s = ms.Batch(cols, consts).run()
-    for i, (v, c) in enumerate(zip(vals, consts)):
-        assert (int(cnt[i]), int(s[i])) == _expect(orc, v, c), i
+    # values around 2^63: for_f and delta_f blocks whose range crosses the
+    # signed boundary (64-bit comparison) next to blocks that do not
+    vf = orc.uniform_bits(7, 16, n) + np.uint64((1 << 63) - 30000)
+    vd = orc.sorted_gaps(8, orc.geom_table(0.25), n) + np.uint64((1 << 63) - 9000)
+    cols += [ms.morph(ms.Column.from_numpy(vf, arena), ms.for_f), ms.morph(ms.Column.from_numpy(vd, arena), ms.delta_f)]
+    vals += [vf, vd]
+    consts += [_median(vf), _median(vd)]
+    for cmp in (O.CMP_LT, O.CMP_LE, O.CMP_GT, O.CMP_GE, O.CMP_EQ):
+        cs = [int(v[len(v) // 3]) if cmp == O.CMP_EQ else c for v, c in zip(vals, consts)]
+        cnt, s = ms.Batch(cols, cs, cmp).run()
+        for i, (v, c) in enumerate(zip(vals, cs)):
+            assert (int(cnt[i]), int(s[i])) == _expect(orc, v, c, cmp), (i, cmp)
 
 
 def test_batch_equals_one_call_per_column(ms, arena, orc):
