@@ -346,4 +346,76 @@ const std::tuple<const column<GrF> *, const column<ExtF> *> group(const column<I
     return std::make_tuple(new column<GrF>(gr), new column<ExtF>(ext));
 }
 
+// --------------------------------------------------------------------------
+// Additions with no single-call counterpart in the reference
+// --------------------------------------------------------------------------
+namespace gpu {
+
+// Many columns in one persistent launch: for every column i, decompress ->
+// select(value t_compare consts[i]) -> sum of the selected values; results are
+// (count, sum) per column.  run() replays a CUDA graph captured on first use.
+template <template <class, int> class t_compare> class select_sum_batch {
+    ms_batch *m_B = nullptr;
+    size_t m_N;
+    void *m_Cnt = nullptr, *m_Sum = nullptr;
+
+public:
+    select_sum_batch(const std::vector<const ms_col *> &cols, const std::vector<uint64_t> &consts) : m_N(cols.size()) {
+        if (consts.size() != cols.size()) throw std::runtime_error("select_sum_batch: one constant per column");
+        std::vector<ms_col> d;
+        for (const ms_col *c : cols) d.push_back(*c);
+        check(ms_gpu_batch_create(d.data(), consts.data(), d.size(), t_compare<void, 64>::code, arena(), &m_B, stream()),
+              "batch_create");
+        check(ms_gpu_arena_alloc(arena(), 8 * (m_N + 1), &m_Cnt), "batch");
+        check(ms_gpu_arena_alloc(arena(), 8 * (m_N + 1), &m_Sum), "batch");
+    }
+    select_sum_batch(const select_sum_batch &) = delete;
+    ~select_sum_batch() { ms_gpu_batch_destroy(m_B); }
+
+    void run(bool graph = true) {
+        check((graph ? ms_gpu_batch_run_graph : ms_gpu_batch_run)(m_B, static_cast<uint64_t *>(m_Cnt),
+                                                                   static_cast<uint64_t *>(m_Sum), stream()),
+              "batch_run");
+    }
+    // (count, sum) per column, after the last run
+    std::vector<std::pair<uint64_t, uint64_t>> results() const {
+        check(ms_gpu_arena_check(arena(), stream()), "batch");
+        std::vector<uint64_t> c(m_N), s(m_N);
+        check(ms_gpu_memcpy(c.data(), m_Cnt, 8 * m_N, 1, 1, stream()), "batch");
+        check(ms_gpu_memcpy(s.data(), m_Sum, 8 * m_N, 1, 1, stream()), "batch");
+        std::vector<std::pair<uint64_t, uint64_t>> r(m_N);
+        for (size_t i = 0; i < m_N; i++) r[i] = {c[i], s[i]};
+        return r;
+    }
+};
+
+// The fused star query: select(filter t_compare c) -> semi_join(dim, fk) ->
+// intersect -> project(gkey, measure) -> group -> grouped agg_sum in one
+// pass; the result equals the operator chain's (keys, extents, sums in
+// group-id order).
+struct star_query_result {
+    std::vector<uint64_t> keys, extents, sums;
+    uint64_t rows;  // |P|, the rows that pass both filters
+};
+
+template <template <class, int> class t_compare, class FF, class KF, class LF, class GF, class MF>
+star_query_result star_query(const column<FF> *filter, uint64_t c, const column<KF> *fk, const column<LF> *dim,
+                             const column<GF> *gkey, const column<MF> *measure, size_t max_groups = 1 << 20) {
+    star_query_result r;
+    r.keys.resize(max_groups);
+    r.extents.resize(max_groups);
+    r.sums.resize(max_groups);
+    uint64_t ng = 0;
+    check(ms_gpu_query3(filter->desc(), t_compare<void, 64>::code, c, fk->desc(), dim->desc(), gkey->desc(),
+                        measure->desc(), max_groups, r.keys.data(), r.extents.data(), r.sums.data(), &ng, &r.rows,
+                        arena(), stream()),
+          "star_query");
+    r.keys.resize(ng);
+    r.extents.resize(ng);
+    r.sums.resize(ng);
+    return r;
+}
+
+}  // namespace gpu
+
 }  // namespace morphstore
