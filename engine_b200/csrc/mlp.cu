@@ -207,24 +207,54 @@ __global__ void __launch_bounds__(128) k_mlp_choose(const float *__restrict__ fe
                                                    const __nv_bfloat16 *__restrict__ wbf, float margin,
                                                    float *__restrict__ pred, uint8_t *__restrict__ choice,
                                                    unsigned long long *__restrict__ nfallback) {
-    __shared__ float W[kP];
+    __shared__ __align__(16) float W[kP];
     for (unsigned i = threadIdx.x; i < kP; i += blockDim.x) W[i] = __bfloat162float(wbf[i]);
     __syncthreads();
     unsigned fb = 0;
+    // The loops are unrolled so x and h1 stay in registers, and the weights
+    // are read four at a time; the order of every sum is the plain loop's.
     for (uint64_t b = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; b < n; b += uint64_t(gridDim.x) * blockDim.x) {
         float x[kIn], h1[kH];
-        for (unsigned k = 0; k < kIn; k++) x[k] = feats[b * kIn + k];
+        const float4 *fx = reinterpret_cast<const float4 *>(feats + b * kIn);
+#pragma unroll
+        for (unsigned k = 0; k < kIn / 4; k++) {
+            const float4 t = __ldg(fx + k);
+            x[4 * k] = t.x;
+            x[4 * k + 1] = t.y;
+            x[4 * k + 2] = t.z;
+            x[4 * k + 3] = t.w;
+        }
+#pragma unroll
         for (unsigned i = 0; i < kH; i++) {
             float z = W[kB1 + i];
-            for (unsigned k = 0; k < kIn; k++) z = fmaf(W[kW1 + i * kIn + k], x[k], z);
+            const float4 *w = reinterpret_cast<const float4 *>(W + kW1 + i * kIn);
+#pragma unroll
+            for (unsigned k = 0; k < kIn / 4; k++) {
+                const float4 t = w[k];
+                z = fmaf(t.x, x[4 * k], z);
+                z = fmaf(t.y, x[4 * k + 1], z);
+                z = fmaf(t.z, x[4 * k + 2], z);
+                z = fmaf(t.w, x[4 * k + 3], z);
+            }
             h1[i] = fmaxf(z, 0.f);
         }
         float o[kOut];
+#pragma unroll
         for (unsigned j = 0; j < kOut; j++) o[j] = W[kB3 + j];
+#pragma unroll 4
         for (unsigned i = 0; i < kH; i++) {
             float z = W[kB2 + i];
-            for (unsigned k = 0; k < kH; k++) z = fmaf(W[kW2 + i * kH + k], h1[k], z);
+            const float4 *w = reinterpret_cast<const float4 *>(W + kW2 + i * kH);
+#pragma unroll
+            for (unsigned k = 0; k < kH / 4; k++) {
+                const float4 t = w[k];
+                z = fmaf(t.x, h1[4 * k], z);
+                z = fmaf(t.y, h1[4 * k + 1], z);
+                z = fmaf(t.z, h1[4 * k + 2], z);
+                z = fmaf(t.w, h1[4 * k + 3], z);
+            }
             z = fmaxf(z, 0.f);
+#pragma unroll
             for (unsigned j = 0; j < kOut; j++) o[j] = fmaf(W[kW3 + j * kH + i], z, o[j]);
         }
         unsigned best = 0;
@@ -364,6 +394,8 @@ extern "C" int ms_gpu_mlp_eval_loss(ms_mlp *m, const float *d_feats, const uint3
 extern "C" int ms_gpu_mlp_choose(ms_mlp *m, const float *d_feats, uint64_t n, float margin_log2, float *d_pred,
                                  uint8_t *d_choice, uint64_t *d_nfallback, void *stream) {
     if (!m || (!d_feats && n)) return ms_fail(MS_ERR_INVALID, "mlp_choose: bad argument");
+    if (reinterpret_cast<uintptr_t>(d_feats) % 16)
+        return ms_fail(MS_ERR_INVALID, "mlp_choose: features must be 16-byte aligned");
     cudaStream_t st = (cudaStream_t)stream;
     if (d_nfallback) MS_CUDA_TRY(cudaMemsetAsync(d_nfallback, 0, 8, st));
     if (!n) return MS_OK;

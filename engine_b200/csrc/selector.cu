@@ -314,7 +314,9 @@ __global__ void __launch_bounds__(256) k_sel_features(const uint64_t *__restrict
     for (uint64_t b = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) / 32; b < nblk;
          b += uint64_t(gridDim.x) * blockDim.x / 32) {
         const uint64_t *x = in + b * kSelBlock;
-        unsigned hv[8] = {0}, hd[8] = {0};
+        // bit-width histograms: eight 8-bit counters per thread in one word
+        // (at most 8 values and 8 deltas per thread)
+        uint64_t hv = 0, hd = 0;
         unsigned vmax = 0, vmin = 64, dmax = 0, neg = 0, heads = 0, zd = 0, vsum = 0, nd = 0;
         unsigned cmax[4] = {0}, cdmax[4] = {0};
         uint64_t umax = 0, umin = ~uint64_t(0);
@@ -334,7 +336,7 @@ __global__ void __launch_bounds__(256) k_sel_features(const uint64_t *__restrict
             for (unsigned u = 0; u < 2; u++) {
                 const uint64_t v = vals[u];
                 const unsigned bw = effective_bitwidth(v);
-                hv[(bw - 1) >> 3]++;
+                hv += uint64_t(1) << (8u * ((bw - 1) >> 3));
                 vmax = max(vmax, bw);
                 vmin = min(vmin, bw);
                 vsum += bw;
@@ -345,7 +347,7 @@ __global__ void __launch_bounds__(256) k_sel_features(const uint64_t *__restrict
             if (lane >= 8) {
                 const uint64_t d = a - a8;
                 const unsigned bw = effective_bitwidth(d);
-                hd[(bw - 1) >> 3]++;
+                hd += uint64_t(1) << (8u * ((bw - 1) >> 3));
                 dmax = max(dmax, bw);
                 cdmax[c] = max(cdmax[c], bw);
                 neg += (int64_t)d < 0;
@@ -355,7 +357,7 @@ __global__ void __launch_bounds__(256) k_sel_features(const uint64_t *__restrict
             {
                 const uint64_t d = bq - b8;
                 const unsigned bw = effective_bitwidth(d);
-                hd[(bw - 1) >> 3]++;
+                hd += uint64_t(1) << (8u * ((bw - 1) >> 3));
                 dmax = max(dmax, bw);
                 cdmax[c] = max(cdmax[c], bw);
                 neg += (int64_t)d < 0;
@@ -367,10 +369,16 @@ __global__ void __launch_bounds__(256) k_sel_features(const uint64_t *__restrict
         }
         float f[kSelNF];
         const float nv = 256.f, ndf = float(__reduce_add_sync(0xFFFFFFFFu, nd));
+        // two counters per 32-bit word (16-bit fields: warp sums stay below 2^16)
 #pragma unroll
-        for (int k = 0; k < 8; k++) {
-            f[k] = float(__reduce_add_sync(0xFFFFFFFFu, hv[k])) / nv;
-            f[8 + k] = float(__reduce_add_sync(0xFFFFFFFFu, hd[k])) / ndf;
+        for (int k = 0; k < 4; k++) {
+            const unsigned pv = unsigned((hv >> (16 * k)) & 0xFFu) | (unsigned((hv >> (16 * k + 8)) & 0xFFu) << 16);
+            const unsigned pd = unsigned((hd >> (16 * k)) & 0xFFu) | (unsigned((hd >> (16 * k + 8)) & 0xFFu) << 16);
+            const unsigned sv = __reduce_add_sync(0xFFFFFFFFu, pv), sd = __reduce_add_sync(0xFFFFFFFFu, pd);
+            f[2 * k] = float(sv & 0xFFFFu) / nv;
+            f[2 * k + 1] = float(sv >> 16) / nv;
+            f[8 + 2 * k] = float(sd & 0xFFFFu) / ndf;
+            f[8 + 2 * k + 1] = float(sd >> 16) / ndf;
         }
         f[16] = float(__reduce_max_sync(0xFFFFFFFFu, vmax)) / 64.f;
         f[17] = float(__reduce_min_sync(0xFFFFFFFFu, vmin)) / 64.f;
