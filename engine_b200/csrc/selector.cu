@@ -75,15 +75,22 @@ __device__ __forceinline__ uint64_t wor(uint64_t x) {
 // Analysis of one block by one warp.  Thread `lane` reads rows
 // j = k*32 + lane (k = 0..63): row j belongs to sub-block k/16 and TVL lane
 // j%8 = lane%8.
+// U: unrolling of the four sub-block rounds (4: all 64 loads of a thread in
+// flight; 1: a quarter of the registers, for kernels that want occupancy).
+template <int U = 4>
 __device__ BlockStats analyze_block(const uint64_t *__restrict__ x, unsigned lane) {
     BlockStats s;
     uint64_t prev = 0;       // x[j - 32] of this thread (previous k)
     uint64_t last_prev = 0;  // x[j - 1] for lane 0: lane 31 of the previous k
     unsigned heads = 0;
-    int64_t mn[2] = {INT64_MAX, INT64_MAX};
-#pragma unroll 4
+    // minima of the two 1024-halves; widths packed one byte per sub-block
+    // (no register arrays indexed by the loop counter)
+    int64_t mn0 = INT64_MAX, mn1 = INT64_MAX;
+    uint32_t raw_p = 0, dlt_p = 0, fr_p = 0;
+#pragma unroll U
     for (unsigned i = 0; i < 4; i++) {
         uint64_t o_raw = 1, o_dlt = 1;
+        int64_t mi = INT64_MAX;
 #pragma unroll
         for (unsigned kk = 0; kk < 16; kk++) {
             const unsigned k = i * 16 + kk;
@@ -97,16 +104,19 @@ __device__ BlockStats analyze_block(const uint64_t *__restrict__ x, unsigned lan
             heads += (k == 0 && lane == 0) ? 1u : unsigned(v != x1);
             o_raw |= v;
             o_dlt |= v - x8;
-            mn[i >> 1] = min(mn[i >> 1], (int64_t)v);
+            mi = min(mi, (int64_t)v);
             last_prev = __shfl_sync(0xFFFFFFFFu, v, 31);
             prev = v;
         }
-        s.raw[i] = uint8_t(effective_bitwidth(wor(o_raw)));
-        s.dlt[i] = uint8_t(effective_bitwidth(wor(o_dlt)));
+        if (i < 2) mn0 = min(mn0, mi);
+        else mn1 = min(mn1, mi);
+        raw_p |= uint32_t(effective_bitwidth(wor(o_raw))) << (8 * i);
+        dlt_p |= uint32_t(effective_bitwidth(wor(o_dlt))) << (8 * i);
     }
     // FOR references: signed minimum per TVL lane, unsigned across lanes
+#pragma unroll
     for (unsigned hh = 0; hh < 2; hh++) {
-        int64_t m = mn[hh];
+        int64_t m = hh ? mn1 : mn0;
         m = min(m, (int64_t)__shfl_xor_sync(0xFFFFFFFFu, (uint64_t)m, 8));
         m = min(m, (int64_t)__shfl_xor_sync(0xFFFFFFFFu, (uint64_t)m, 16));
         uint64_t um = (uint64_t)m;
@@ -117,13 +127,19 @@ __device__ BlockStats analyze_block(const uint64_t *__restrict__ x, unsigned lan
         s.ref[hh] = um;
     }
     // FOR offsets (second read of the block, from L1/L2)
-#pragma unroll 4
+#pragma unroll U
     for (unsigned i = 0; i < 4; i++) {
         uint64_t o = 1;
-        const uint64_t ref = s.ref[i >> 1];
+        const uint64_t ref = i < 2 ? s.ref[0] : s.ref[1];
 #pragma unroll
         for (unsigned kk = 0; kk < 16; kk++) o |= __ldg(x + (i * 16 + kk) * 32 + lane) - ref;
-        s.fr[i] = uint8_t(effective_bitwidth(wor(o)));
+        fr_p |= uint32_t(effective_bitwidth(wor(o))) << (8 * i);
+    }
+#pragma unroll
+    for (unsigned i = 0; i < 4; i++) {
+        s.raw[i] = uint8_t(raw_p >> (8 * i));
+        s.dlt[i] = uint8_t(dlt_p >> (8 * i));
+        s.fr[i] = uint8_t(fr_p >> (8 * i));
     }
     s.runs = __reduce_add_sync(0xFFFFFFFFu, heads);
     s.sbw = uint8_t(max(max(s.raw[0], s.raw[1]), max(s.raw[2], s.raw[3])));
@@ -158,14 +174,20 @@ __global__ void __launch_bounds__(256) k_sel_analyze(const uint64_t *__restrict_
 
 // Exhaustive decision for the blocks the learned selector left open
 // (choice 255); the others keep their choice.
-__global__ void __launch_bounds__(256) k_sel_resolve(const uint64_t *__restrict__ in, uint64_t nblk,
-                                                    uint8_t *__restrict__ choice) {
+// A warp reads the choices of its next 32 blocks (one per lane) in one go
+// and analyses only the open ones.
+__global__ void __launch_bounds__(256, 2) k_sel_resolve(const uint64_t *__restrict__ in, uint64_t nblk,
+                                                       uint8_t *__restrict__ choice) {
     const unsigned lane = threadIdx.x & 31u;
-    for (uint64_t b = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) / 32; b < nblk;
-         b += uint64_t(gridDim.x) * blockDim.x / 32) {
-        if (choice[b] != 255) continue;
-        const BlockStats s = analyze_block(in + b * kSelBlock, lane);
-        if (lane == 0) choice[b] = uint8_t(best_cand(s));
+    const uint64_t W = uint64_t(gridDim.x) * blockDim.x / 32;
+    for (uint64_t b0 = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) / 32; b0 < nblk; b0 += 32 * W) {
+        const uint64_t mine = b0 + lane * W;
+        const bool open = mine < nblk && choice[mine] == 255;
+        for (unsigned todo = __ballot_sync(0xFFFFFFFFu, open); todo; todo &= todo - 1) {
+            const uint64_t b = b0 + uint64_t(__ffs(todo) - 1) * W;
+            const BlockStats s = analyze_block<1>(in + b * kSelBlock, lane);
+            if (lane == 0) choice[b] = uint8_t(best_cand(s));
+        }
     }
 }
 
