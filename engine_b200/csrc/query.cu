@@ -182,11 +182,14 @@ __host__ __device__ inline uint64_t q3_meta_bytes(unsigned S) {
     return (uint64_t(16) * S + sizeof(QStage) * S + 5ull * kQCols * S * kQTile + 127) / 128 * 128;
 }
 
-template <int W>
+// kSB: the build side's bitmap (nwords words) is copied into shared memory
+// after the group table, so the probes cost a shared-memory load instead of
+// an L2 round trip.
+template <int W, bool kSB>
 __global__ void __launch_bounds__(32 * (W + 1), 1)
     k_query3_tma(ColView fk, ColView gkey, ColView meas, StreamCol c0, StreamCol c1, StreamCol c2, StreamCol c3,
-                 Pred pred, const uint32_t *__restrict__ bits, uint64_t lo, uint64_t span, QCfg cfg, GTable gt,
-                 uint32_t *__restrict__ blk_hits, unsigned *err) {
+                 Pred pred, const uint32_t *__restrict__ bits, uint64_t nwords, uint64_t lo, uint64_t span, QCfg cfg,
+                 GTable gt, uint32_t *__restrict__ blk_hits, unsigned *err) {
     extern __shared__ __align__(128) uint8_t smem[];
     const unsigned S = cfg.stages, SB = cfg.stage_bytes;
     uint64_t *full = reinterpret_cast<uint64_t *>(smem);
@@ -199,12 +202,16 @@ __global__ void __launch_bounds__(32 * (W + 1), 1)
     unsigned long long *s_first = s_key + kQSlots;
     unsigned long long *s_sum = s_first + kQSlots;
 
+    uint32_t *s_bits = reinterpret_cast<uint32_t *>(s_sum + kQSlots);
+    const uint32_t *pbits = kSB ? s_bits : bits;
     const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     for (unsigned i = threadIdx.x; i < kQSlots; i += blockDim.x) {
         s_key[i] = kQEmpty;
         s_first[i] = ~0ull;
         s_sum[i] = 0;
     }
+    if (kSB)
+        for (uint64_t i = threadIdx.x; i < nwords; i += blockDim.x) s_bits[i] = __ldg(bits + i);
     if (threadIdx.x == 0) {
         for (unsigned st = 0; st < S; st++) {
             mbar_init(full + st, 1);
@@ -344,7 +351,7 @@ __global__ void __launch_bounds__(32 * (W + 1), 1)
                             const uint64_t v = vbp_extract(kb, kbw, l, 16u * q + kk[i]) + kref;
                             const uint64_t d = v - lo;
                             inr[i] = had[i] && v >= lo && d < span;
-                            word[i] = inr[i] ? __ldg(bits + (d >> 5)) : 0u;
+                            word[i] = inr[i] ? (kSB ? pbits[d >> 5] : __ldg(pbits + (d >> 5))) : 0u;
                             bit[i] = unsigned(d & 31u);
                         }
 #pragma unroll
@@ -504,33 +511,46 @@ __global__ void __launch_bounds__(256) k_q3_extents(GTable gt, ColView filt, Col
 
 bool random_access(const ColView &v) { return plain(v) || v.fmt == MS_FMT_FOR_DVBP; }
 
+constexpr size_t kQSmemMax = 232448;  // 227 KiB of dynamic shared memory per CTA
+
 // launch configuration of the staged kernel (consumer warps 8/16/24)
 ms_tuning g_q3 = {1, 16, 3, 57344, 1, 16};
 
 template <int W>
-int launch_q3_tma_w(const ColView &fv, const ColView &kv, const ColView &gv, const ColView &mv, const StreamCol &s0,
-                    const StreamCol &s1, const StreamCol &s2, const StreamCol &s3, const Pred &pred,
-                    const uint32_t *bits, uint64_t lo, uint64_t span, const GTable &gt, uint32_t *hits,
-                    unsigned *d_err, cudaStream_t st) {
+int launch_q3_tma_w(const ColView &kv, const ColView &gv, const ColView &mv, const StreamCol &s0, const StreamCol &s1,
+                    const StreamCol &s2, const StreamCol &s3, const Pred &pred, const uint32_t *bits, uint64_t nwords,
+                    uint64_t lo, uint64_t span, const GTable &gt, uint32_t *hits, unsigned *d_err, cudaStream_t st) {
     const QCfg cfg{g_q3.stages, g_q3.stage_bytes};
-    const size_t shm = q3_meta_bytes(cfg.stages) + size_t(cfg.stages) * cfg.stage_bytes + 3ull * 8 * kQSlots;
-    auto kern = k_query3_tma<W>;
-    MS_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
-    kern<<<unsigned(sm_count()), 32 * (W + 1), shm, st>>>(kv, gv, mv, s0, s1, s2, s3, pred, bits, lo, span, cfg,
-                                                          gt, hits, d_err);
+    const size_t table = 3ull * 8 * kQSlots, bitmap = 4 * nwords;
+    size_t shm = q3_meta_bytes(cfg.stages) + size_t(cfg.stages) * cfg.stage_bytes + table;
+    // The bitmap goes to shared memory when it fits beside the ring.  (Shrinking
+    // the ring to make room for a large bitmap was measured slower: a 2^20-key
+    // build side with a 2 x 25 KiB ring lost more to the shallower pipeline
+    // than the probes gained.)
+    const bool sb = g_q3.staged == 1 && shm + bitmap <= kQSmemMax;
+    shm = q3_meta_bytes(cfg.stages) + size_t(cfg.stages) * cfg.stage_bytes + table + (sb ? bitmap : 0);
+    if (sb) {
+        auto kern = k_query3_tma<W, true>;
+        MS_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
+        kern<<<unsigned(sm_count()), 32 * (W + 1), shm, st>>>(kv, gv, mv, s0, s1, s2, s3, pred, bits, nwords, lo,
+                                                              span, cfg, gt, hits, d_err);
+    } else {
+        auto kern = k_query3_tma<W, false>;
+        MS_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
+        kern<<<unsigned(sm_count()), 32 * (W + 1), shm, st>>>(kv, gv, mv, s0, s1, s2, s3, pred, bits, nwords, lo,
+                                                              span, cfg, gt, hits, d_err);
+    }
     MS_CUDA_TRY(cudaGetLastError());
-    (void)fv;
     return MS_OK;
 }
 
-int launch_q3_tma(const ColView &fv, const ColView &kv, const ColView &gv, const ColView &mv, const StreamCol &s0,
-                  const StreamCol &s1, const StreamCol &s2, const StreamCol &s3, const Pred &pred,
-                  const uint32_t *bits, uint64_t lo, uint64_t span, const GTable &gt, uint32_t *hits,
-                  unsigned *d_err, cudaStream_t st) {
+int launch_q3_tma(const ColView &kv, const ColView &gv, const ColView &mv, const StreamCol &s0, const StreamCol &s1,
+                  const StreamCol &s2, const StreamCol &s3, const Pred &pred, const uint32_t *bits, uint64_t nwords,
+                  uint64_t lo, uint64_t span, const GTable &gt, uint32_t *hits, unsigned *d_err, cudaStream_t st) {
     switch (g_q3.warps) {
-    case 8: return launch_q3_tma_w<8>(fv, kv, gv, mv, s0, s1, s2, s3, pred, bits, lo, span, gt, hits, d_err, st);
-    case 24: return launch_q3_tma_w<24>(fv, kv, gv, mv, s0, s1, s2, s3, pred, bits, lo, span, gt, hits, d_err, st);
-    default: return launch_q3_tma_w<16>(fv, kv, gv, mv, s0, s1, s2, s3, pred, bits, lo, span, gt, hits, d_err, st);
+    case 8: return launch_q3_tma_w<8>(kv, gv, mv, s0, s1, s2, s3, pred, bits, nwords, lo, span, gt, hits, d_err, st);
+    case 24: return launch_q3_tma_w<24>(kv, gv, mv, s0, s1, s2, s3, pred, bits, nwords, lo, span, gt, hits, d_err, st);
+    default: return launch_q3_tma_w<16>(kv, gv, mv, s0, s1, s2, s3, pred, bits, nwords, lo, span, gt, hits, d_err, st);
     }
 }
 
@@ -540,11 +560,14 @@ int launch_q3_tma(const ColView &fv, const ColView &kv, const ColView &gv, const
 using namespace ms;
 
 // Launch configuration of the fused query's staged kernel: staged (0 = the
-// direct kernel only), warps (consumer warps: 8, 16 or 24), stages and
+// direct kernel only, 1 = staged with the build-side bitmap in shared memory
+// when it fits, 2 = staged with the bitmap in global memory), warps
+// (consumer warps: 8, 16 or 24), stages and
 // stage_bytes (shared-memory ring; stages x stage_bytes + 48 KiB group table
 // must fit 227 KiB).  The other fields are ignored.
 extern "C" int ms_gpu_set_query_tuning(const ms_tuning *t) {
     if (!t) return ms_fail(MS_ERR_INVALID, "set_query_tuning: null");
+    if (t->staged > 2) return ms_fail(MS_ERR_INVALID, "set_query_tuning: staged must be 0, 1 or 2");
     if (t->warps != 8 && t->warps != 16 && t->warps != 24)
         return ms_fail(MS_ERR_INVALID, "set_query_tuning: warps must be 8, 16 or 24");
     if (t->stages < 2 || t->stages > 16 || t->stage_bytes % 128 || t->stage_bytes < 16384)
@@ -638,8 +661,8 @@ extern "C" int ms_gpu_query3(const ms_col *filter, int cmp, uint64_t c, const ms
                 const StreamCol s0 = stream_of(fv), s1 = stream_of(kv), s2 = stream_of(gv), s3 = stream_of(mv);
                 nbs = minu(minu(s0.nb, s1.nb), minu(s2.nb, s3.nb));
                 if (nbs) {
-                    rc = launch_q3_tma(fv, kv, gv, mv, s0, s1, s2, s3, make_pred(cmp, c), bits, lo, span, gt, hits,
-                                       a->d_err, st);
+                    rc = launch_q3_tma(kv, gv, mv, s0, s1, s2, s3, make_pred(cmp, c), bits, words, lo, span, gt,
+                                       hits, a->d_err, st);
                     if (rc) return rc;
                 }
             }

@@ -33,8 +33,11 @@ FILTER_LT = 400
 DIM_KEYS = 1 << 20
 
 
-QUERY_CONFIGS = [dict(staged=0)] + [dict(staged=1, warps=w, stages=s, stage_bytes=b)
-                                    for w in (8, 16, 24) for s, b in ((2, 81920), (3, 57344), (4, 40960), (6, 27648))]
+# staged=1 keeps the build side's bitmap in shared memory when it fits beside
+# the ring, staged=2 always reads it from global memory
+QUERY_CONFIGS = [dict(staged=0)] + [dict(staged=st, warps=w, stages=s, stage_bytes=b)
+                                    for st in (1, 2) for w in (8, 16, 24)
+                                    for s, b in ((2, 81920), (3, 57344), (4, 40960), (6, 27648))]
 
 
 def run(log2_rows: int = 28, reps: int = 5, sweep: bool = False) -> dict:

@@ -232,7 +232,9 @@ int ms_gpu_query3(const ms_col *filter, int cmp, uint64_t c, const ms_col *fk, c
                   uint64_t *h_ext, uint64_t *h_sums, uint64_t *n_groups, uint64_t *n_rows_p,
                   ms_arena *arena, void *stream);
 /* Launch configuration of ms_gpu_query3's staged kernel (no counterpart in
- * the reference): staged (0 = direct kernel only), warps (consumer warps 8,
+ * the reference): staged (0 = direct kernel only, 1 = staged with the
+ * build side's bitmap in shared memory when it fits, 2 = staged with the
+ * bitmap in global memory), warps (consumer warps 8,
  * 16 or 24), stages, stage_bytes; other fields ignored.  Rejects a ring that
  * does not fit shared memory with the 48 KiB group table. */
 int ms_gpu_set_query_tuning(const ms_tuning *t);

@@ -127,7 +127,8 @@ def test_query3_rejects_bad_input(ms, arena, orc):
         ms.query3(r, O.CMP_LT, 5, a, a, a, a)
 
 
-@pytest.mark.parametrize("cfg", [dict(staged=0), dict(warps=8, stages=2, stage_bytes=16384),
+@pytest.mark.parametrize("cfg", [dict(staged=0), dict(staged=2, warps=16, stages=3, stage_bytes=57344),
+                                 dict(warps=8, stages=2, stage_bytes=16384),
                                  dict(warps=16, stages=4, stage_bytes=40960),
                                  dict(warps=24, stages=3, stage_bytes=57344)])
 def test_query3_launch_configs(ms, arena, orc, cfg):
