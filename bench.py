@@ -314,6 +314,15 @@ def run_gpu(args):
         t = torch.tensor([total_ms], device=dev)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         total_ms = float(t.item())
+        # the shards' results combined once (outside the timed region): the
+        # query over the whole table is the sum of the per-shard sums
+        def s64(v):
+            return v - (1 << 64) if v >= 1 << 63 else v
+        comb = torch.tensor([s64(got_sum), got_cnt, s64(exp_sum), exp_cnt, int(not ok)], dtype=torch.int64,
+                            device=dev)
+        torch.distributed.all_reduce(comb)
+        ok = bool(comb[4].item() == 0 and comb[0].item() == comb[2].item() and comb[1].item() == comb[3].item())
+        got_cnt = int(comb[1].item())
     ms_per_step = total_ms / args.steps
     kern_ms = statistics.mean(per)
     value = world * algo_bytes / (ms_per_step * 1e-3) / 1e9
@@ -327,7 +336,8 @@ def run_gpu(args):
             "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "rows_per_gpu": n, "compressed_bytes_per_gpu": algo_bytes,
-                       "parallelism": f"replicas{world}" if world > 1 else "single",
+                       "parallelism": f"shards{world} (one per rank, results combined by all_reduce)"
+                       if world > 1 else "single",
                        "l2": "inputs (1.0 GB) larger than L2; no flush",
                        "launch": dict(ms.get_tuning(), source="tuning.json" if tuned else "default")},
             "parity": {"sum_ok": ok, "count": got_cnt},
