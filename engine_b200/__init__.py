@@ -87,6 +87,8 @@ _sig = {
     "ms_gpu_set_tuning": (C.c_int, [_P(MsTuning)]),
     "ms_gpu_set_query_tuning": (C.c_int, [_P(MsTuning)]),
     "ms_gpu_col_compact": (C.c_int, [_P(MsCol), _P(MsCol), _V, _V]),
+    "ms_col_store": (C.c_int, [_P(MsCol), C.c_char_p, _V]),
+    "ms_col_load": (C.c_int, [C.c_char_p, C.c_int, C.c_uint, _P(MsCol), _V, _V]),
     "ms_gpu_batch_create": (C.c_int, [_P(MsCol), _V, _U64, C.c_int, _V, _P(_V), _V]),
     "ms_gpu_batch_set_config": (C.c_int, [_V, _P(MsTuning)]),
     "ms_gpu_batch_get_config": (C.c_int, [_V, _P(MsTuning)]),
@@ -325,6 +327,20 @@ class Column:
             pa = self.arena.alloc(aux.nbytes)
             _memcpy_h2d(pa, aux)
             self.desc.index_aux = pa
+
+    def store(self, path: str, stream=None) -> None:
+        """binary_io<F>::store (binary_io.h:72-84): [count][used bytes][bytes]."""
+        _check(_lib.ms_col_store(C.byref(self.desc), os.fsencode(path), _stream_ptr(stream)), "col_store")
+
+    @staticmethod
+    def load(path: str, fmt: "Format", arena: "Arena | None" = None, stream=None) -> "Column":
+        """binary_io<F>::load (binary_io.h:43-70) into device memory."""
+        arena = arena or default_arena()
+        fmt = _fmt(fmt)
+        out = MsCol()
+        _check(_lib.ms_col_load(os.fsencode(path), fmt.code, fmt.bw, C.byref(out), arena.h, _stream_ptr(stream)),
+               "col_load")
+        return Column(out, arena)
 
     def compact(self, arena: "Arena | None" = None, stream=None) -> "Column":
         """A copy of this column in storage of exactly its used size."""

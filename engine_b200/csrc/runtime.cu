@@ -3,6 +3,9 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <cstdio>
+#include <vector>
+
 #include "internal.h"
 #include "scan.cuh"
 
@@ -45,9 +48,9 @@ extern "C" int ms_gpu_get_tuning(ms_tuning *t) {
 }
 
 extern "C" const char *ms_gpu_status_string(int status) {
-    static const char *names[] = {"MS_OK",          "MS_ERR_INVALID", "MS_ERR_UNSUPPORTED", "MS_ERR_CUDA",
-                                  "MS_ERR_NOMEM",   "MS_ERR_CORRUPT", "MS_ERR_TIMEOUT"};
-    if (status < 0 || status > 6) return "MS_ERR_UNKNOWN";
+    static const char *names[] = {"MS_OK",        "MS_ERR_INVALID", "MS_ERR_UNSUPPORTED", "MS_ERR_CUDA",
+                                  "MS_ERR_NOMEM", "MS_ERR_CORRUPT", "MS_ERR_TIMEOUT",     "MS_ERR_IO"};
+    if (status < 0 || status > 7) return "MS_ERR_UNKNOWN";
     return status == MS_OK ? names[0] : (g_last_error[0] ? g_last_error : names[status]);
 }
 
@@ -372,6 +375,102 @@ extern "C" int ms_gpu_col_compact(const ms_col *in, ms_col *out, ms_arena *a, vo
     c.index = index;
     c.index_aux = aux;
     if (!index) c.n_index = 0;
+    *out = c;
+    return MS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// persistence: binary_io<F> (binary_io.h:40-87)
+// ---------------------------------------------------------------------------
+extern "C" int ms_col_store(const ms_col *c, const char *path, void *stream) {
+    using namespace ms;
+    if (!c || !path) return ms_fail(MS_ERR_INVALID, "col_store: null argument");
+    int rc = check_col(c, false);
+    if (rc) return rc;
+    std::vector<uint8_t> h(c->size_used_byte);
+    if (!h.empty()) {
+        MS_CUDA_TRY(cudaMemcpyAsync(h.data(), c->data, h.size(), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+        MS_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+    }
+    FILE *f = std::fopen(path, "wb");
+    if (!f) return ms_fail(MS_ERR_IO, "col_store: could not open the file for writing");
+    const uint64_t meta[2] = {c->count_values, c->size_used_byte};
+    bool ok = std::fwrite(meta, 8, 2, f) == 2 && (h.empty() || std::fwrite(h.data(), 1, h.size(), f) == h.size());
+    ok = (std::fclose(f) == 0) && ok;
+    return ok ? MS_OK : ms_fail(MS_ERR_IO, "col_store: could not write the column meta data and data");
+}
+
+extern "C" int ms_col_load(const char *path, int fmt, unsigned bw, ms_col *out, ms_arena *a, void *stream) {
+    using namespace ms;
+    if (!path || !out || !a) return ms_fail(MS_ERR_INVALID, "col_load: null argument");
+    if (fmt < MS_FMT_UNCOMPR || fmt > MS_FMT_RLE || (fmt == MS_FMT_STATIC_VBP && (bw < 1 || bw > 64)))
+        return ms_fail(MS_ERR_INVALID, "col_load: format");
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return ms_fail(MS_ERR_IO, "col_load: could not open the file for reading");
+    uint64_t meta[2] = {0, 0};
+    if (std::fread(meta, 8, 2, f) != 2) {
+        std::fclose(f);
+        return ms_fail(MS_ERR_IO, "col_load: could not read the column meta data");
+    }
+    const uint64_t count = meta[0], used = meta[1];
+    if (used > (uint64_t(1) << 40)) {
+        std::fclose(f);
+        return ms_fail(MS_ERR_CORRUPT, "col_load: implausible column size");
+    }
+    std::vector<uint8_t> h(used + 64, 0);
+    const bool ok = used == 0 || std::fread(h.data(), 1, used, f) == used;
+    std::fclose(f);
+    if (!ok) return ms_fail(MS_ERR_IO, "col_load: could not read the column data");
+    // the compressed size, recovered from the format
+    uint64_t compr = 0, ncompr = 0;
+    std::vector<uint64_t> idx, aux;
+    if (fmt == MS_FMT_RLE) {
+        compr = used;
+        if (used % 16) return ms_fail(MS_ERR_CORRUPT, "col_load: rle_f size is not a multiple of 16");
+    } else if (fmt == MS_FMT_STATIC_VBP) {
+        ncompr = count - count % kBlock;
+        compr = ncompr / 8 * bw;
+    } else if (fmt != MS_FMT_UNCOMPR) {
+        const uint64_t blk = fmt == MS_FMT_DYNAMIC_VBP ? kBlock : 2 * kBlock;
+        ncompr = count - count % blk;
+        const uint64_t nb = ncompr / kBlock;
+        if (nb) {
+            idx.resize(nb + 1);
+            aux.resize(nb / 2 + 1);
+            int rc = ms_host_build_index(fmt, h.data(), used, ncompr, idx.data(),
+                                         fmt == MS_FMT_FOR_DVBP ? aux.data() : nullptr);
+            if (rc) return rc;
+            compr = idx_off(idx[nb - 1]) + 64ull * idx_bw(idx[nb - 1]);
+        }
+    }
+    const uint64_t nrest = count - ncompr;
+    const uint64_t expect = fmt == MS_FMT_UNCOMPR ? 8 * count
+                            : fmt == MS_FMT_RLE ? used
+                            : (nrest ? rest_offset(fmt, bw, compr) + 8 * nrest : compr);
+    if (expect != used) return ms_fail(MS_ERR_CORRUPT, "col_load: stored size disagrees with the format");
+    ms_col c{};
+    c.format = uint32_t(fmt);
+    c.bw = fmt == MS_FMT_STATIC_VBP ? bw : 0;
+    c.count_values = count;
+    c.size_used_byte = used;
+    c.size_compr_byte = fmt == MS_FMT_UNCOMPR ? 0 : compr;
+    c.size_alloc_byte = used + 64;
+    c.data = arena_take_t<uint8_t>(a, used + 64);
+    if (!c.data) return ms_fail(MS_ERR_NOMEM, "arena exhausted (col_load)");
+    cudaStream_t st = (cudaStream_t)stream;
+    MS_CUDA_TRY(cudaMemcpyAsync(c.data, h.data(), used + 64, cudaMemcpyHostToDevice, st));
+    if (!idx.empty()) {
+        const uint64_t nb = idx.size() - 1;
+        uint64_t *di = arena_take_t<uint64_t>(a, nb + 1);
+        uint64_t *da = fmt == MS_FMT_FOR_DVBP ? arena_take_t<uint64_t>(a, nb / 2 + 1) : nullptr;
+        if (!di || (fmt == MS_FMT_FOR_DVBP && !da)) return ms_fail(MS_ERR_NOMEM, "arena exhausted (col_load index)");
+        MS_CUDA_TRY(cudaMemcpyAsync(di, idx.data(), 8 * nb, cudaMemcpyHostToDevice, st));
+        if (da) MS_CUDA_TRY(cudaMemcpyAsync(da, aux.data(), 8 * (nb / 2 + 1), cudaMemcpyHostToDevice, st));
+        c.index = di;
+        c.index_aux = da;
+        c.n_index = nb;
+    }
+    MS_CUDA_TRY(cudaStreamSynchronize(st));
     *out = c;
     return MS_OK;
 }

@@ -347,6 +347,22 @@ const std::tuple<const column<GrF> *, const column<ExtF> *> group(const column<I
 }
 
 // --------------------------------------------------------------------------
+// binary_io<F> (include/core/persistence/binary_io.h:40-87): the same file
+// layout, columns loaded into device memory
+// --------------------------------------------------------------------------
+template <class F> class binary_io {
+public:
+    static const column<F> *load(const std::string &p_Filename) {
+        ms_col d{};
+        gpu::check(ms_col_load(p_Filename.c_str(), F::ms_code, F::ms_bw, &d, gpu::arena(), gpu::stream()), "load");
+        return new column<F>(d);
+    }
+    static void store(const column<F> *p_Column, const std::string &p_FileName) {
+        gpu::check(ms_col_store(p_Column->desc(), p_FileName.c_str(), gpu::stream()), "store");
+    }
+};
+
+// --------------------------------------------------------------------------
 // Additions with no single-call counterpart in the reference
 // --------------------------------------------------------------------------
 namespace gpu {

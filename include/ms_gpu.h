@@ -41,7 +41,8 @@ typedef enum ms_status {
     MS_ERR_CUDA = 3,         /* a CUDA runtime call failed                      */
     MS_ERR_NOMEM = 4,        /* arena or output capacity exhausted              */
     MS_ERR_CORRUPT = 5,      /* a kernel found an invalid header / bit width    */
-    MS_ERR_TIMEOUT = 6       /* a bounded device-side wait gave up              */
+    MS_ERR_TIMEOUT = 6,      /* a bounded device-side wait gave up              */
+    MS_ERR_IO = 7            /* a column file could not be read or written      */
 } ms_status;
 
 enum {
@@ -144,6 +145,17 @@ int ms_gpu_build_index(ms_col *col, ms_arena *arena, void *stream);
  * (get_size_max_byte_any_len, format.h:114-153), so a column that is kept
  * can be compacted after it is produced.  Asynchronous. */
 int ms_gpu_col_compact(const ms_col *in, ms_col *out, ms_arena *arena, void *stream);
+
+/* ---- persistence (binary_io<F>, include/core/persistence/binary_io.h:40-87)
+ * File layout as the reference's: [count_values u64][size_used_byte u64]
+ * [size_used_byte bytes of the column buffer].  store copies the column to
+ * the host and writes it (synchronous); load reads it, recovers the
+ * compressed size from the format (page walk for the dynamic_vbp family,
+ * which also builds the block index), checks that it agrees with the stored
+ * size and uploads the column into the arena.  `format`/`bw` name the
+ * column's format, as binary_io<F>'s template argument does. */
+int ms_col_store(const ms_col *col, const char *path, void *stream);
+int ms_col_load(const char *path, int format, unsigned bw, ms_col *out, ms_arena *arena, void *stream);
 
 /* ---- operators (include/core/operators/interfaces/) ----------------------- */
 /* agg_sum<ve,F>(col) (agg_sum.h:56-65; agg_sum_compr.h:78-153): the uint64

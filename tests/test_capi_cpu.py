@@ -62,3 +62,18 @@ def test_host_index_matches_layout(orc):
             off, bw = int(idx[blk]) & ((1 << 56) - 1), int(idx[blk]) >> 56
             words = b[off: off + 64 * bw].view(np.uint64)
             assert len(words) == 8 * bw
+
+
+def test_col_load_reports_missing_file(tmp_path):
+    """binary_io load of a file that does not exist fails before touching the
+    device, with the I/O status."""
+    import ctypes as C
+    import engine_b200 as ms
+    out = ms.MsCol()
+    rc = ms.lib().ms_col_load(str(tmp_path / "missing.bin").encode(), ms.DYNAMIC_VBP, 0, C.byref(out), None, None)
+    assert rc == 1  # null arena is rejected first
+    arena_stub = C.c_void_p(1)  # never dereferenced: the file is opened first
+    rc = ms.lib().ms_col_load(str(tmp_path / "missing.bin").encode(), ms.DYNAMIC_VBP, 0, C.byref(out), arena_stub,
+                              None)
+    assert rc == 7
+    assert b"could not open" in ms.lib().ms_gpu_status_string(rc)
