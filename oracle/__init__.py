@@ -85,6 +85,8 @@ class Oracle:
         L.orc_select_project_sum.argtypes = [C.c_int, C.c_uint64, U64P, U64P, C.c_uint64, C.c_uint64, U64P]
         L.orc_semi_join.restype = C.c_uint64
         L.orc_semi_join.argtypes = [U64P, C.c_uint64, U64P, C.c_uint64, U64P]
+        L.orc_natural_join.restype = C.c_uint64
+        L.orc_natural_join.argtypes = [U64P, C.c_uint64, U64P, C.c_uint64, U64P, U64P]
         L.orc_intersect_sorted.restype = C.c_uint64
         L.orc_intersect_sorted.argtypes = [U64P, C.c_uint64, U64P, C.c_uint64, U64P]
         L.orc_group.restype = C.c_uint64
@@ -187,6 +189,15 @@ class Oracle:
         k = self.lib.orc_semi_join(lp, len(l), rp, len(r), out.ctypes.data_as(U64P))
         return out[:k].copy()
 
+    def natural_join(self, l, r):
+        """(build positions, probe positions) of the natural equi-join."""
+        l, lp = _u64(l)
+        r, rp = _u64(r)
+        ol = np.zeros(max(len(r), 1), dtype=np.uint64)
+        orr = np.zeros(max(len(r), 1), dtype=np.uint64)
+        k = self.lib.orc_natural_join(lp, len(l), rp, len(r), ol.ctypes.data_as(U64P), orr.ctypes.data_as(U64P))
+        return ol[:k].copy(), orr[:k].copy()
+
     def intersect_sorted(self, l, r):
         l, lp = _u64(l)
         r, rp = _u64(r)
@@ -278,6 +289,8 @@ class Reference:
         L.ref_agg_sum.argtypes = [C.c_int, C.c_uint, U8P, M, U64P]
         L.ref_semi_join.argtypes = [C.c_int, U8P, M, C.c_int, U8P, M, C.c_int, U8P, C.c_uint64, M]
         L.ref_intersect.argtypes = [C.c_int, U8P, M, U64P, C.c_uint64, C.c_int, U8P, C.c_uint64, M]
+        L.ref_natural_join.argtypes = [C.c_int, U8P, M, C.c_int, U8P, M, C.c_int, U8P, C.c_uint64, M, U8P,
+                                       C.c_uint64, M]
         L.ref_intersect_scalar.restype = C.c_uint64
         L.ref_intersect_scalar.argtypes = [U64P, C.c_uint64, U64P, C.c_uint64, U64P]
         L.ref_group.argtypes = [C.c_int, U8P, M, C.c_int, U8P, C.c_uint64, M, C.c_int, U8P, C.c_uint64, M]
@@ -359,6 +372,22 @@ class Reference:
         if rc:
             raise ValueError(f"ref_semi_join rc={rc}")
         return out[: mo.size_used_byte].copy(), mo.tuple()
+
+    def natural_join(self, l_fmt, l, lmeta, r_fmt, r, rmeta, out_fmt):
+        """join<ve, out, out, L_f, R_f>(L, R): ((bytes, meta) of the build
+        positions, (bytes, meta) of the probe positions)."""
+        lp, rp = self._padded(l), self._padded(r)
+        cap = self._cap(rmeta[0])
+        ol = np.zeros(cap, dtype=np.uint8)
+        orr = np.zeros(cap, dtype=np.uint8)
+        ml, mr = Meta(), Meta()
+        rc = self.lib.ref_natural_join(l_fmt, lp.ctypes.data_as(U8P), C.byref(Meta(*lmeta)), r_fmt,
+                                       rp.ctypes.data_as(U8P), C.byref(Meta(*rmeta)), out_fmt,
+                                       ol.ctypes.data_as(U8P), cap, C.byref(ml), orr.ctypes.data_as(U8P), cap,
+                                       C.byref(mr))
+        if rc:
+            raise ValueError(f"ref_natural_join rc={rc}")
+        return (ol[: ml.size_used_byte].copy(), ml.tuple()), (orr[: mr.size_used_byte].copy(), mr.tuple())
 
     def intersect(self, l_fmt, l, lmeta, r_values, out_fmt):
         lp = self._padded(l)

@@ -501,6 +501,50 @@ uint64_t orc_semi_join(const uint64_t *l, uint64_t nl, const uint64_t *r, uint64
     return k;
 }
 
+/* natural equi-join (join_natural_equi_compr.h:116-300 with the hash_map of
+ * join.h:158-187): the build side L maps each key to the position of its
+ * first occurrence (an insert of a key already present keeps the old value,
+ * linear_probing.h:315-366); every probe row of R whose value is a key emits
+ * (L position, R position), in R order.  Returns the number of pairs. */
+typedef struct {
+    uint64_t key, pos;
+} orc_kp;
+
+static int cmp_kp(const void *a, const void *b) {
+    const orc_kp *x = (const orc_kp *)a, *y = (const orc_kp *)b;
+    if (x->key != y->key) return x->key < y->key ? -1 : 1;
+    return x->pos < y->pos ? -1 : (x->pos > y->pos);
+}
+
+uint64_t orc_natural_join(const uint64_t *l, uint64_t nl, const uint64_t *r, uint64_t nr, uint64_t *out_l,
+                          uint64_t *out_r) {
+    orc_kp *m = (orc_kp *)malloc(sizeof(orc_kp) * (nl ? nl : 1));
+    for (uint64_t i = 0; i < nl; i++) {
+        m[i].key = l[i];
+        m[i].pos = i;
+    }
+    qsort(m, nl, sizeof(orc_kp), cmp_kp);
+    uint64_t u = 0;  /* keep the first position of every key */
+    for (uint64_t i = 0; i < nl; i++)
+        if (i == 0 || m[i].key != m[u - 1].key) m[u++] = m[i];
+    uint64_t k = 0;
+    for (uint64_t j = 0; j < nr; j++) {
+        uint64_t lo = 0, hi = u;
+        while (lo < hi) {
+            const uint64_t mid = lo + (hi - lo) / 2;
+            if (m[mid].key < r[j]) lo = mid + 1;
+            else hi = mid;
+        }
+        if (lo < u && m[lo].key == r[j]) {
+            out_l[k] = m[lo].pos;
+            out_r[k] = j;
+            k++;
+        }
+    }
+    free(m);
+    return k;
+}
+
 /* intersect_sorted (scalar/intersect_uncompr.h:41-86) */
 uint64_t orc_intersect_sorted(const uint64_t *l, uint64_t nl, const uint64_t *r, uint64_t nr, uint64_t *out) {
     uint64_t i = 0, j = 0, k = 0;

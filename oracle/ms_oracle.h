@@ -82,6 +82,8 @@ uint64_t orc_select_project_sum(int cmp, uint64_t c, const uint64_t *x, const ui
                                 uint64_t n, uint64_t scalar_from, uint64_t *count);
 uint64_t orc_semi_join(const uint64_t *l, uint64_t nl, const uint64_t *r, uint64_t nr,
                        uint64_t *out_pos);
+uint64_t orc_natural_join(const uint64_t *l, uint64_t nl, const uint64_t *r, uint64_t nr, uint64_t *out_l,
+                          uint64_t *out_r);
 uint64_t orc_intersect_sorted(const uint64_t *l, uint64_t nl, const uint64_t *r,
                               uint64_t nr, uint64_t *out);
 uint64_t orc_group(const uint64_t *gr_in, const uint64_t *data, uint64_t n,

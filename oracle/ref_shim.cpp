@@ -20,6 +20,7 @@
 #include <core/operators/general_vectorized/agg_sum_compr.h>
 #include <core/operators/general_vectorized/group_compr.h>
 #include <core/operators/general_vectorized/join_semi_equi_compr.h>
+#include <core/operators/general_vectorized/join_natural_equi_compr.h>
 #include <core/operators/general_vectorized/intersect_compr.h>
 #include <core/operators/interfaces/join.h>
 #if defined(PART_OPS)
@@ -92,6 +93,9 @@ using IsL = flist<uf, dv, dd>;
 using IsOut = flist<uf, dv>;
 using GrIn = flist<uf, dv>;
 using GrOut = flist<uf, dv>;
+using JnL = flist<uf, dd>;
+using JnR = flist<uf, dv, fd>;
+using JnOut = flist<uf, dv>;
 
 template <class F> static const column<F> *make_col(const uint8_t *bytes, const ref_meta *m, uint64_t alloc) {
     auto *c = new column<F>(alloc + 64);
@@ -421,6 +425,37 @@ uint64_t ref_bench_select_project_sum(const uint64_t *x, const uint64_t *y, uint
     return sum;
 }
 
+#endif
+
+#if defined(PART_JOIN)
+// join<ve, outL_f, outR_f, L_f, R_f>(L, R) (join.h:158-187): the natural
+// equi-join, (build position, probe position) pairs in probe order; both
+// outputs in the same format.
+int ref_natural_join(int l_fmt, const uint8_t *l, const ref_meta *lm, int r_fmt, const uint8_t *r, const ref_meta *rm,
+                     int out_fmt, uint8_t *out_l, uint64_t cap_l, ref_meta *om_l, uint8_t *out_r, uint64_t cap_r,
+                     ref_meta *om_r) {
+    return with_formats<JnL>(l_fmt, 0, [&](auto tl) {
+        using FL = typename decltype(tl)::type;
+        const column<FL> *lc = make_col<FL>(l, lm, alloc_for<FL>(lm));
+        int res = with_formats<JnR>(r_fmt, 0, [&](auto tr) {
+            using FR = typename decltype(tr)::type;
+            const column<FR> *rc = make_col<FR>(r, rm, alloc_for<FR>(rm));
+            int r2 = with_formats<JnOut>(out_fmt, 0, [&](auto to) {
+                using FO = typename decltype(to)::type;
+                auto res2 = join<ve, FO, FO, FL, FR>(lc, rc);
+                int r3 = export_col(std::get<0>(res2), out_l, cap_l, om_l);
+                if (!r3) r3 = export_col(std::get<1>(res2), out_r, cap_r, om_r);
+                delete std::get<0>(res2);
+                delete std::get<1>(res2);
+                return r3;
+            });
+            delete rc;
+            return r2;
+        });
+        delete lc;
+        return res;
+    });
+}
 #endif
 
 }  // extern "C"

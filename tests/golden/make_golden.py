@@ -118,6 +118,18 @@ def main():
         ob, om = ref.semi_join(O.DELTA_DVBP, lb, lm, O.FOR_DVBP, rb, rm, out_fmt)
         fx[f"semi/{out_fmt}/bytes"] = O.mask_gap(out_fmt, 0, ob, om, orc)
         fx[f"semi/{out_fmt}/meta"] = np.array(om, dtype=np.uint64)
+    # --- natural equi-join (duplicate build keys: the first position wins) -------------------
+    lk = orc.uniform_bits(12, 11, 4000)
+    rk = orc.uniform_bits(13, 12, 30_011)
+    fx["njoin/l"], fx["njoin/r"] = lk, rk
+    lb, lm = ref.compress(O.DELTA_DVBP, 0, lk)
+    rb, rm = ref.compress(O.FOR_DVBP, 0, rk)
+    for out_fmt in (O.UNCOMPR, O.DYNAMIC_VBP):
+        (ob, om), (pb, pm) = ref.natural_join(O.DELTA_DVBP, lb, lm, O.FOR_DVBP, rb, rm, out_fmt)
+        fx[f"njoin/{out_fmt}/l/bytes"] = O.mask_gap(out_fmt, 0, ob, om, orc)
+        fx[f"njoin/{out_fmt}/l/meta"] = np.array(om, dtype=np.uint64)
+        fx[f"njoin/{out_fmt}/r/bytes"] = O.mask_gap(out_fmt, 0, pb, pm, orc)
+        fx[f"njoin/{out_fmt}/r/meta"] = np.array(pm, dtype=np.uint64)
     # --- intersect -----------------------------------------------------------------------
     a = np.flatnonzero(orc.uniform_bits(8, 3, 20_000) < 3).astype(np.uint64)
     b2 = np.flatnonzero(orc.uniform_bits(9, 3, 20_000) < 5).astype(np.uint64)

@@ -82,6 +82,20 @@ def test_semi_join(orc):
         assert np.array_equal(O.mask_gap(out_fmt, 0, b, m, orc), FX[f"semi/{out_fmt}/bytes"])
 
 
+def test_natural_join(orc):
+    """The oracle's natural equi-join, written through the write-iterator
+    model, reproduces the reference's two output columns byte for byte."""
+    lpos, rpos = orc.natural_join(FX["njoin/l"], FX["njoin/r"])
+    rm = orc.compress(O.FOR_DVBP, 0, FX["njoin/r"])[1]
+    sf = orc.scalar_from(O.FOR_DVBP, 0, rm)
+    nscal = int((rpos >= sf).sum())
+    for out_fmt in (O.UNCOMPR, O.DYNAMIC_VBP):
+        for side, vals in (("l", lpos), ("r", rpos)):
+            b, m = orc.wi_write(out_fmt, 0, vals, nscal)
+            assert tuple(int(v) for v in FX[f"njoin/{out_fmt}/{side}/meta"]) == m, (out_fmt, side)
+            assert np.array_equal(O.mask_gap(out_fmt, 0, b, m, orc), FX[f"njoin/{out_fmt}/{side}/bytes"]), (out_fmt, side)
+
+
 def test_intersect(orc):
     assert np.array_equal(orc.intersect_sorted(FX["isect/l"], FX["isect/r"]), FX["isect/out"])
 
