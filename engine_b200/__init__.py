@@ -87,6 +87,8 @@ _sig = {
     "ms_gpu_set_tuning": (C.c_int, [_P(MsTuning)]),
     "ms_gpu_set_query_tuning": (C.c_int, [_P(MsTuning)]),
     "ms_gpu_col_compact": (C.c_int, [_P(MsCol), _P(MsCol), _V, _V]),
+    "ms_gpu_natural_join": (C.c_int, [_P(MsCol), _P(MsCol), C.c_int, C.c_uint, C.c_int, C.c_uint, _P(MsCol),
+                                      _P(MsCol), _V, _V]),
     "ms_col_store": (C.c_int, [_P(MsCol), C.c_char_p, _V]),
     "ms_col_load": (C.c_int, [C.c_char_p, C.c_int, C.c_uint, _P(MsCol), _V, _V]),
     "ms_gpu_batch_create": (C.c_int, [_P(MsCol), _V, _U64, C.c_int, _V, _P(_V), _V]),
@@ -436,6 +438,16 @@ def semi_join(l: Column, r: Column, out_f: Format = uncompr_f, stream=None) -> C
     _check(_lib.ms_gpu_semi_join(C.byref(l.desc), C.byref(r.desc), out_f.code, out_f.bw, C.byref(out), r.arena.h,
                                  _stream_ptr(stream)), "semi_join")
     return Column(out, r.arena, keep=(l, r))
+
+
+def natural_join(l: Column, r: Column, out_l_f: Format = uncompr_f, out_r_f: Format = uncompr_f, stream=None):
+    """join<ve, outL_f, outR_f, L_f, R_f>(L, R) (join.h:158-187): (positions
+    in L of the first occurrence of each matching value, rows of R)."""
+    fl, fr = _fmt(out_l_f), _fmt(out_r_f)
+    ol, orr = MsCol(), MsCol()
+    _check(_lib.ms_gpu_natural_join(C.byref(l.desc), C.byref(r.desc), fl.code, fl.bw, fr.code, fr.bw, C.byref(ol),
+                                    C.byref(orr), r.arena.h, _stream_ptr(stream)), "natural_join")
+    return Column(ol, r.arena, keep=(l, r)), Column(orr, r.arena, keep=(l, r))
 
 
 def intersect_sorted(l: Column, r: Column, out_f: Format = uncompr_f, stream=None) -> Column:

@@ -171,6 +171,120 @@ __global__ void __launch_bounds__(256) k_probe(ColView r, KeySet s, uint32_t *__
     if (!ok) atomicOr(err, kErrCorrupt);
 }
 
+// ---------------------------------------------------------------------------
+// Natural equi-join (join_natural_equi_compr.h:116-300): the build side maps
+// every key to the position of its first occurrence (the reference's hash
+// map keeps the value of the first insert, linear_probing.h:315-366).  Dense
+// key ranges use a direct array of positions, others an open-addressing
+// table; both are filled with atomicMin, so the result does not depend on the
+// order in which warps insert.
+// ---------------------------------------------------------------------------
+struct KeyMap {
+    unsigned long long *dense;  // dense mode: position per key - lo (~0: absent)
+    uint64_t lo, span;
+    unsigned long long *keys;   // hash mode
+    unsigned long long *vals;
+    uint64_t mask;
+    unsigned long long *max_pos;  // position of key 2^64-1 (it doubles as the empty marker)
+};
+
+__device__ __forceinline__ uint64_t map_lookup(const KeyMap &m, uint64_t k) {
+    if (m.dense) {
+        const uint64_t d = k - m.lo;
+        return (k < m.lo || d >= m.span) ? kEmpty : m.dense[d];
+    }
+    if (k == kEmpty) return *m.max_pos;
+    uint64_t h = hash64(k) & m.mask;
+    for (uint64_t probe = 0; probe <= m.mask; probe++) {
+        const uint64_t v = m.keys[h];
+        if (v == k) return m.vals[h];
+        if (v == kEmpty) return kEmpty;
+        h = (h + 1) & m.mask;
+    }
+    return kEmpty;
+}
+
+__global__ void k_build_map(ColView c, KeyMap m, unsigned *err) {
+    const unsigned lane = threadIdx.x & 31u, l = lane & 7u, q = lane >> 3;
+    bool ok = true;
+    for (uint64_t b = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) / 32; b < c.nblocks_total();
+         b += uint64_t(gridDim.x) * blockDim.x / 32) {
+        uint64_t v[16];
+        unsigned valid;
+        ok &= decode_block(c, b, l, q, v, valid);
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+            if (!((valid >> k) & 1u)) continue;
+            const uint64_t key = v[k];
+            const unsigned long long row = b * kBlock + (16u * q + k) * 8u + l;
+            if (m.dense) {
+                atomicMin(m.dense + (key - m.lo), row);
+                continue;
+            }
+            if (key == kEmpty) {
+                atomicMin(m.max_pos, row);
+                continue;
+            }
+            uint64_t h = hash64(key) & m.mask;
+            bool placed = false;
+            for (uint64_t probe = 0; probe <= m.mask; probe++) {
+                const unsigned long long old = atomicCAS(m.keys + h, (unsigned long long)kEmpty, (unsigned long long)key);
+                if (old == kEmpty || old == key) {
+                    atomicMin(m.vals + h, row);
+                    placed = true;
+                    break;
+                }
+                h = (h + 1) & m.mask;
+            }
+            if (!placed) atomicOr(err, kErrCapacity);
+        }
+    }
+    if (!ok) atomicOr(err, kErrCorrupt);
+}
+
+// Probe: per block, hits = rows of r whose value is a key.  Pass 1
+// (blk_off == nullptr) stores per-block counts, pass 2 writes the pairs.
+__global__ void __launch_bounds__(256) k_probe_map(ColView r, KeyMap m, uint32_t *__restrict__ blk_counts,
+                                                  const uint64_t *__restrict__ blk_off, uint64_t *__restrict__ out_r,
+                                                  uint64_t *__restrict__ out_l,
+                                                  unsigned long long *__restrict__ d_scalar_hits, unsigned *err) {
+    const unsigned lane = threadIdx.x & 31u, l = lane & 7u, q = lane >> 3;
+    bool ok = true;
+    for (uint64_t b = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) / 32; b < r.nblocks_total();
+         b += uint64_t(gridDim.x) * blockDim.x / 32) {
+        uint64_t v[16];
+        unsigned valid;
+        ok &= decode_block(r, b, l, q, v, valid);
+        unsigned mk = 0;
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+            const uint64_t p = ((valid >> k) & 1u) ? map_lookup(m, v[k]) : kEmpty;
+            v[k] = p;  // the build position replaces the value
+            mk |= unsigned(p != kEmpty) << k;
+        }
+        if (!blk_off) {
+            const unsigned tot = __reduce_add_sync(0xFFFFFFFFu, __popc(mk));
+            if (lane == 0) blk_counts[b] = tot;
+            continue;
+        }
+        if (!__any_sync(0xFFFFFFFFu, mk != 0)) continue;
+        unsigned rank[16];
+        block_ranks(mk, l, q, rank);
+        const uint64_t base = blk_off[b], row0 = b * kBlock;
+        unsigned scal = 0;
+#pragma unroll
+        for (int k = 0; k < 16; k++)
+            if ((mk >> k) & 1u) {
+                const uint64_t row = row0 + (16u * q + k) * 8u + l;
+                out_r[base + rank[k]] = row;
+                out_l[base + rank[k]] = v[k];
+                scal += row >= r.sfrom;
+            }
+        if (scal) atomicAdd(d_scalar_hits, (unsigned long long)scal);
+    }
+    if (!ok) atomicOr(err, kErrCorrupt);
+}
+
 // intersect: rows of l (a sorted position list) whose value occurs in the
 // sorted array rv; pass structure as k_probe, output = the values.
 __global__ void __launch_bounds__(256) k_intersect(ColView lc, const uint64_t *__restrict__ rv, uint64_t nr,
@@ -700,3 +814,85 @@ extern "C" int ms_gpu_agg_sum_grouped(const ms_col *gr, const ms_col *data, uint
     out->data = res;
     return MS_OK;
 }
+
+// join<ve, outL_f, outR_f, L_f, R_f>(L, R) (join.h:158-187,
+// join_natural_equi_compr.h:116-300): (build position, probe position)
+// pairs in probe order; the two outputs follow the write iterator model in
+// their formats.
+extern "C" int ms_gpu_natural_join(const ms_col *l, const ms_col *r, int out_l_format, unsigned out_l_bw,
+                                   int out_r_format, unsigned out_r_bw, ms_col *out_l, ms_col *out_r, ms_arena *a,
+                                   void *stream) {
+    if (!l || !r || !out_l || !out_r || !a) return ms_fail(MS_ERR_INVALID, "natural_join: null argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    ColView lv, rv;
+    int rc = view_or_decompress(l, a, st, &lv);
+    if (rc) return rc;
+    rc = view_or_decompress(r, a, st, &rv);
+    if (rc) return rc;
+    unsigned long long *mm = arena_take_t<unsigned long long>(a, 3);
+    if (!mm) return ms_fail(MS_ERR_NOMEM, "arena exhausted (natural_join)");
+    const unsigned long long init[3] = {~0ull, 0ull, ~0ull};
+    MS_CUDA_TRY(cudaMemcpyAsync(mm, init, 24, cudaMemcpyHostToDevice, st));
+    const uint64_t nbl = lv.nblocks_total(), nl = l->count_values;
+    if (nbl) {
+        k_minmax<<<grid_blocks(nbl), 256, 0, st>>>(lv, mm, mm + 1, a->d_err);
+        MS_CUDA_TRY(cudaGetLastError());
+    }
+    unsigned long long hmm[2];
+    MS_CUDA_TRY(cudaMemcpyAsync(hmm, mm, 16, cudaMemcpyDeviceToHost, st));
+    MS_CUDA_TRY(cudaStreamSynchronize(st));
+    KeyMap m{};
+    m.max_pos = mm + 2;
+    if (nl && hmm[1] - hmm[0] < (uint64_t(1) << 24)) {
+        m.lo = hmm[0];
+        m.span = hmm[1] - hmm[0] + 1;
+        m.dense = arena_take_t<unsigned long long>(a, m.span);
+        if (!m.dense) return ms_fail(MS_ERR_NOMEM, "arena exhausted (natural_join array)");
+        MS_CUDA_TRY(cudaMemsetAsync(m.dense, 0xFF, 8 * m.span, st));
+    } else {
+        uint64_t cap = 16;
+        while (cap < 2 * nl) cap <<= 1;
+        m.keys = arena_take_t<unsigned long long>(a, cap);
+        m.vals = arena_take_t<unsigned long long>(a, cap);
+        if (!m.keys || !m.vals) return ms_fail(MS_ERR_NOMEM, "arena exhausted (natural_join table)");
+        MS_CUDA_TRY(cudaMemsetAsync(m.keys, 0xFF, 8 * cap, st));
+        MS_CUDA_TRY(cudaMemsetAsync(m.vals, 0xFF, 8 * cap, st));
+        m.mask = cap - 1;
+    }
+    if (nbl) {
+        k_build_map<<<grid_blocks(nbl), 256, 0, st>>>(lv, m, a->d_err);
+        MS_CUDA_TRY(cudaGetLastError());
+    }
+    // two passes over the probe side: counts, scan, pairs
+    const uint64_t nbt = rv.nblocks_total();
+    uint32_t *bc = arena_take_t<uint32_t>(a, nbt + 1);
+    uint64_t *bo = arena_take_t<uint64_t>(a, nbt + 1);
+    uint64_t *tot = arena_take_t<uint64_t>(a, 2);
+    uint64_t *scr = arena_take_t<uint64_t>(a, scan_scratch_words(nbt, 1));
+    if (!bc || !bo || !tot || !scr) return ms_fail(MS_ERR_NOMEM, "arena exhausted (natural_join)");
+    MS_CUDA_TRY(cudaMemsetAsync(tot, 0, 16, st));
+    if (nbt) {
+        k_probe_map<<<grid_blocks(nbt), 256, 0, st>>>(rv, m, bc, nullptr, nullptr, nullptr, nullptr, a->d_err);
+        MS_CUDA_TRY(cudaGetLastError());
+        MS_CUDA_TRY((scan_exclusive<uint32_t, 1>(bc, nbt, bo, tot, scr, st)));
+    }
+    uint64_t total = 0;
+    MS_CUDA_TRY(cudaMemcpyAsync(&total, tot, 8, cudaMemcpyDeviceToHost, st));
+    MS_CUDA_TRY(cudaStreamSynchronize(st));
+    uint64_t *pr = arena_take_t<uint64_t>(a, total + 1);
+    uint64_t *pl = arena_take_t<uint64_t>(a, total + 1);
+    if (!pr || !pl) return ms_fail(MS_ERR_NOMEM, "arena exhausted (natural_join output)");
+    if (total) {
+        k_probe_map<<<grid_blocks(nbt), 256, 0, st>>>(rv, m, bc, bo, pr, pl, (unsigned long long *)(tot + 1),
+                                                      a->d_err);
+        MS_CUDA_TRY(cudaGetLastError());
+    }
+    uint64_t scal = 0;
+    MS_CUDA_TRY(cudaMemcpyAsync(&scal, tot + 1, 8, cudaMemcpyDeviceToHost, st));
+    rc = read_err(a, st);
+    if (rc) return rc;
+    rc = write_values(pl, total - scal, scal, out_l_format, out_l_bw, out_l, a, st);
+    if (rc) return rc;
+    return write_values(pr, total - scal, scal, out_r_format, out_r_bw, out_r, a, st);
+}
+

@@ -315,6 +315,17 @@ const column<OutF> *intersect_sorted(const column<LF> *l, const column<RF> *r, s
     return new column<OutF>(out);
 }
 
+// natural equi-join (join.h:158-187): (build positions, probe positions)
+template <class VE, class OutLF, class OutRF, class LF, class RF>
+const std::tuple<const column<OutLF> *, const column<OutRF> *> join(const column<LF> *l, const column<RF> *r,
+                                                                    size_t = 0) {
+    ms_col ol{}, orr{};
+    gpu::check(ms_gpu_natural_join(l->desc(), r->desc(), OutLF::ms_code, OutLF::ms_bw, OutRF::ms_code, OutRF::ms_bw,
+                                   &ol, &orr, gpu::arena(), gpu::stream()),
+               "join");
+    return std::make_tuple(new column<OutLF>(ol), new column<OutRF>(orr));
+}
+
 template <class VE, class OutF, class LF, class RF> struct my_intersect_wit_t {
     static const column<OutF> *apply(const column<LF> *l, const column<RF> *r, size_t est = 0) {
         return intersect_sorted<VE, OutF, LF, RF>(l, r, est);

@@ -196,6 +196,15 @@ int ms_gpu_select_project_sum_async(const ms_col *x, int cmp, uint64_t c, const 
 int ms_gpu_semi_join(const ms_col *l, const ms_col *r, int out_format, unsigned out_bw,
                      ms_col *out, ms_arena *arena, void *stream);
 
+/* join<ve, outL_f, outR_f, L_f, R_f>(L, R) (include/core/operators/
+ * interfaces/join.h:158-187, general_vectorized/join_natural_equi_compr.h:
+ * 116-300): the natural equi-join of build side L and probe side R; out_l
+ * receives, for every row of R (in order) whose value occurs in L, the
+ * position of that value's first occurrence in L, out_r the row of R.  Both
+ * outputs in their formats (write-iterator model). */
+int ms_gpu_natural_join(const ms_col *l, const ms_col *r, int out_l_format, unsigned out_l_bw, int out_r_format,
+                        unsigned out_r_bw, ms_col *out_l, ms_col *out_r, ms_arena *arena, void *stream);
+
 /* intersect_sorted / my_intersect_wit_t (intersect.h:52-63,
  * intersect_compr.h:190-347): sorted intersection of two position lists. */
 int ms_gpu_intersect_sorted(const ms_col *l, const ms_col *r, int out_format, unsigned out_bw,

@@ -75,3 +75,18 @@ def test_semi_join_intersect_group(ms, arena, orc):
         assert np.array_equal(O.mask_gap(O.DYNAMIC_VBP, 0, col.raw_bytes(), m, orc), FX[key + "/bytes"]), key
     s = ms.agg_sum_grouped(gr, ms.Column.from_numpy(FX["group/meas"], arena), ext.get_count_values())
     assert np.array_equal(s.to_numpy(), FX["group/sum"])
+
+
+def test_natural_join_golden(ms, arena, orc):
+    """Both output columns of the reference's natural join, byte for byte
+    (delta+dvbp build side, for+dvbp probe side, uncompr and dvbp outputs)."""
+    lc = ms.morph(ms.Column.from_numpy(FX["njoin/l"], arena), ms.delta_f)
+    rc = ms.morph(ms.Column.from_numpy(FX["njoin/r"], arena), ms.for_f)
+    for out_fmt in (O.UNCOMPR, O.DYNAMIC_VBP):
+        ol, orr = ms.natural_join(lc, rc, F(ms, out_fmt), F(ms, out_fmt))
+        for side, col in (("l", ol), ("r", orr)):
+            m = tuple(int(v) for v in FX[f"njoin/{out_fmt}/{side}/meta"])
+            assert col.meta() == m, (out_fmt, side)
+            assert np.array_equal(O.mask_gap(out_fmt, 0, col.raw_bytes(), m, orc),
+                                  FX[f"njoin/{out_fmt}/{side}/bytes"]), (out_fmt, side)
+

@@ -120,3 +120,42 @@ def test_group_then_sum_pipeline(ms, arena, orc):
     s = ms.agg_sum_grouped(gr, _col(ms, arena, orc, meas, O.DYNAMIC_VBP), ext.get_count_values())
     egr, eext = orc.group(keys)
     assert np.array_equal(s.to_numpy(), orc.agg_sum_grouped(egr, meas, len(eext)))
+
+
+@pytest.mark.parametrize("l_code", [O.UNCOMPR, O.DYNAMIC_VBP, O.DELTA_DVBP, O.RLE])
+@pytest.mark.parametrize("r_code", [O.UNCOMPR, O.DYNAMIC_VBP, O.FOR_DVBP])
+@pytest.mark.parametrize("outs", [(O.UNCOMPR, O.UNCOMPR), (O.DYNAMIC_VBP, O.DELTA_DVBP)])
+def test_natural_join(ms, arena, orc, l_code, r_code, outs):
+    """Build keys with duplicates (the first position is kept), probe rows
+    that miss, odd lengths; outputs in their formats."""
+    lk = orc.uniform_bits(21, 12, 9_000 + 3)
+    if l_code == O.RLE:
+        lk = orc.runs(21, 3, 12, 9_000 + 3)
+    rk = orc.uniform_bits(22, 13, 50_000 + 11)
+    lc = ms.morph(ms.Column.from_numpy(lk, arena), F(ms, l_code)) if l_code != O.UNCOMPR else \
+        ms.Column.from_numpy(lk, arena)
+    rc = _col(ms, arena, orc, rk, r_code)
+    ol, orr = ms.natural_join(lc, rc, F(ms, outs[0]), F(ms, outs[1]))
+    el, er = orc.natural_join(lk, rk)
+    sf = orc.scalar_from(r_code, 0, rc.meta())
+    nscal = int((er >= sf).sum())
+    for col, vals, code in ((ol, el, outs[0]), (orr, er, outs[1])):
+        b, m = orc.wi_write(code, 0, vals, nscal)
+        assert col.meta() == m
+        assert np.array_equal(col.to_numpy(), vals)
+
+
+def test_natural_join_hash_path_and_edges(ms, arena, orc):
+    """Keys spanning more than 2^24 values use the hash table, including the
+    key 2^64-1; an empty build side or probe side gives empty outputs."""
+    lk = np.concatenate([orc.uniform_bits(31, 64, 4000), np.array([2 ** 64 - 1, 7, 7], np.uint64)])
+    rk = np.concatenate([lk[::5], orc.uniform_bits(32, 64, 20_000), np.array([2 ** 64 - 1, 7], np.uint64)])
+    rk = rk[orc.uniform_bits(33, 64, len(rk)).argsort(kind="stable")]
+    ol, orr = ms.natural_join(ms.Column.from_numpy(lk, arena), ms.Column.from_numpy(rk, arena))
+    el, er = orc.natural_join(lk, rk)
+    assert np.array_equal(ol.to_numpy(), el) and np.array_equal(orr.to_numpy(), er)
+    empty = ms.Column.from_numpy(np.zeros(0, np.uint64), arena)
+    for a, b in ((empty, ms.Column.from_numpy(rk, arena)), (ms.Column.from_numpy(lk, arena), empty)):
+        ol, orr = ms.natural_join(a, b)
+        assert ol.get_count_values() == 0 and orr.get_count_values() == 0
+
