@@ -226,18 +226,71 @@ __global__ void __launch_bounds__(32 * W, 1)
     // consumer state: delta carry of lane l (threads (l, q) all hold it)
     uint64_t carry = 0;
 
+    // Look-ahead: the next item is taken off the queue and its description
+    // and block locations loaded one step per issued tile, so the chain of
+    // dependent loads (queue atomic -> item -> column -> block index) overlaps
+    // the current item's copies instead of stalling the warp between items.
+    enum : unsigned { kLaNone = 0, kLaId = 1, kLaItem = 2, kLaCol = 3, kLaReady = 4, kLaEmpty = 5 };
+    unsigned la = kLaNone;
+    unsigned long long la_id = 0;  // lane 0 holds the atomic's result until it is broadcast
+    BItem la_bi{};
+    const uint64_t *la_index = nullptr;
+    unsigned la_cbw = 0;
+    const uint8_t *la_data = nullptr;
+    uint64_t la_off = 0;
+    unsigned la_bw = 0;
+    auto la_step = [&]() {
+        if (la == kLaNone) {
+            if (lane == 0) la_id = atomicAdd(head, 1ull);
+            la = kLaId;
+        } else if (la == kLaId) {
+            la_id = __shfl_sync(0xFFFFFFFFu, la_id, 0);
+            if (la_id >= n_items) {
+                la = kLaEmpty;
+                return;
+            }
+            la_bi = items[la_id];
+            la = kLaItem;
+        } else if (la == kLaItem) {
+            if (la_bi.kind <= kItDelta) {
+                const BCol &c = cols[la_bi.col];
+                la_index = c.index;
+                la_cbw = c.bw;
+                la_data = c.data;
+            }
+            la = kLaCol;
+        } else if (la == kLaCol) {
+            la_off = 0;
+            la_bw = 0;
+            if (la_bi.kind <= kItDelta && lane < la_bi.count) {
+                if (la_index) {
+                    const uint64_t e = __ldg(la_index + la_bi.start + lane);
+                    la_off = idx_off(e);
+                    la_bw = idx_bw(e);
+                } else {
+                    la_bw = la_cbw;
+                    la_off = (la_bi.start + lane) * 64ull * la_cbw;
+                }
+            }
+            la = kLaReady;
+        }
+    };
+
     auto issue = [&]() {
         if (it_left == 0) {
-            unsigned long long id = 0;
-            if (lane == 0) id = atomicAdd(head, 1ull);
-            id = __shfl_sync(0xFFFFFFFFu, id, 0);
-            if (id >= n_items) {
+            while (la != kLaReady && la != kLaEmpty) la_step();  // finish the look-ahead if it is behind
+            if (la == kLaEmpty) {
                 exhausted = true;
                 return;
             }
-            it = uint32_t(id);
-            const BItem bi = items[id];
+            it = uint32_t(la_id);
+            const BItem bi = la_bi;
             it_col = bi.col;
+            it_data = la_data;
+            it_off = la_off;
+            it_bw = la_bw;
+            la = kLaNone;
+            la_step();  // request the following item now
             if (bi.kind == kItRest || bi.kind == kItRle) {  // read in place: no copy
                 const unsigned s = issued % S;
                 if (lane == 0) {
@@ -252,21 +305,8 @@ __global__ void __launch_bounds__(32 * W, 1)
             }
             it_start = it_next = bi.start;
             it_left = bi.count;
-            // the item's block locations, one lane per block, kept for all its tiles
-            const BCol &c = cols[it_col];
-            it_data = c.data;
-            it_off = 0;
-            it_bw = 0;
-            if (lane < it_left) {
-                if (c.index) {
-                    const uint64_t e = __ldg(c.index + bi.start + lane);
-                    it_off = idx_off(e);
-                    it_bw = idx_bw(e);
-                } else {
-                    it_bw = c.bw;
-                    it_off = (bi.start + lane) * 64ull * c.bw;
-                }
-            }
+        } else if (la != kLaReady && la != kLaEmpty) {
+            la_step();
         }
         const unsigned s = issued % S;
         const unsigned k0 = unsigned(it_next - it_start);  // first block of the tile within the item
@@ -318,35 +358,40 @@ __global__ void __launch_bounds__(32 * W, 1)
         const BCol &c = cols[bi.col];
         const uint8_t *base = ring + size_t(s) * SBw;
         uint64_t cnt = 0, sum = 0;
-        if (bi.kind == kItVbp) {
-            for (unsigned j = 0; j < sd.nblk; j++) {
-                const uint64_t *blk = reinterpret_cast<const uint64_t *>(base + sd.off[j]);
-                unsigned k = 0;
-                sum += self_sum_block_rt(sd.bw[j], blk, l, q, c.pred, k, bad);
-                cnt += k;
-            }
-        } else if (bi.kind == kItFor) {
-            for (unsigned j = 0; j < sd.nblk; j++) {
+        if (bi.kind == kItVbp || bi.kind == kItFor) {
+            // two blocks at a time, one per half-warp, 32 values per thread
+            const unsigned hb = lane >> 4, h = (lane >> 3) & 1u;
+            for (unsigned j0 = 0; j0 < sd.nblk; j0 += 2) {
+                const unsigned j = j0 + hb;
+                if (j >= sd.nblk) continue;  // the second half-warp when the tile has an odd count
                 const uint64_t *blk = reinterpret_cast<const uint64_t *>(base + sd.off[j]);
                 const unsigned bw = sd.bw[j];
+                if (bi.kind == kItVbp) {
+                    unsigned k = 0;
+                    sum += self_sum32_block_rt(bw, blk, l, h, c.pred, k, bad);
+                    cnt += k;
+                    continue;
+                }
                 const uint64_t ref = __ldg(c.aux + ((sd.b0 + j) >> 1));
                 Pred pd;
                 if (bw <= 32 && rel_pred(ref, uint64_t(1) << bw, c.c, c.pred.cmp, pd)) {
                     // values ref + d: select and sum on d in the bit-width switch
                     unsigned k = 0;
-                    const uint64_t sd_ = self_sum_block_rt(bw, blk, l, q, pd, k, bad);
+                    const uint64_t sd_ = self_sum32_block_rt(bw, blk, l, h, pd, k, bad);
                     cnt += k;
                     sum += sd_ + uint64_t(k) * ref;
                 } else {
-                    uint64_t v[16];
-                    bad |= !vbp_decode16_rt<true>(bw, blk, l, q, v);
                     // every row of the compressed part precedes the scalar remainder
+                    for (unsigned qq = 2 * h; qq < 2 * h + 2; qq++) {
+                        uint64_t v[16];
+                        bad |= !vbp_decode16_rt<true>(bw, blk, l, qq, v);
 #pragma unroll
-                    for (int k = 0; k < 16; k++) {
-                        const uint64_t x = v[k] + ref;
-                        const bool hit = cmp_bits(x, c.c, c.cf, true);
-                        cnt += hit;
-                        sum += hit ? x : 0;
+                        for (int k = 0; k < 16; k++) {
+                            const uint64_t x = v[k] + ref;
+                            const bool hit = cmp_bits(x, c.c, c.cf, true);
+                            cnt += hit;
+                            sum += hit ? x : 0;
+                        }
                     }
                 }
             }

@@ -414,3 +414,59 @@ __device__ __forceinline__ uint64_t self_sum_block_rt(unsigned bw, const uint64_
 }
 
 }  // namespace ms
+
+namespace ms {
+
+// self_sum_block with 32 values per thread: thread (l, h) of a half-warp
+// takes slots 32h..32h+31 of lane l (word-aligned half streams); wider
+// blocks fall back to the 16-value form on quarters 2h and 2h+1.
+template <unsigned BW>
+__device__ __forceinline__ uint64_t self_sum32_block(const uint64_t *blk, unsigned l, unsigned h, const Pred &p,
+                                                     unsigned &cnt) {
+    if (BW <= 32) {
+        uint32_t v[32];
+        vbp_decode32_u32<(BW <= 32 ? BW : 32)>(blk, l, h, v);
+        unsigned m = 0;
+        if (p.is_eq) {
+            const bool in = p.val < (uint64_t(1) << 32);
+            const uint32_t c = uint32_t(p.val);
+#pragma unroll
+            for (int k = 0; k < 32; k++) m |= unsigned(in && v[k] == c) << k;
+        } else {
+            const bool big = p.T > 0xFFFFFFFFull;
+            const uint32_t T = uint32_t(p.T);
+#pragma unroll
+            for (int k = 0; k < 32; k++) m |= unsigned(big || v[k] < T) << k;
+            if (p.flip) m = ~m;
+        }
+        cnt = __popc(m);
+        if (BW <= 26) {  // 32 values of < 2^26 fit a 32-bit partial sum
+            uint32_t s = 0;
+#pragma unroll
+            for (int k = 0; k < 32; k++) s += ((m >> k) & 1u) ? v[k] : 0u;
+            return s;
+        }
+        uint64_t s = 0;
+#pragma unroll
+        for (int k = 0; k < 32; k++) s += ((m >> k) & 1u) ? v[k] : 0u;
+        return s;
+    } else {
+        unsigned c0 = 0, c1 = 0;
+        const uint64_t s = self_sum_block<BW>(blk, l, 2 * h, p, c0) + self_sum_block<BW>(blk, l, 2 * h + 1, p, c1);
+        cnt = c0 + c1;
+        return s;
+    }
+}
+
+__device__ __forceinline__ uint64_t self_sum32_block_rt(unsigned bw, const uint64_t *blk, unsigned l, unsigned h,
+                                                        const Pred &p, unsigned &cnt, bool &bad) {
+    switch (bw) {
+#define MS_X(B) \
+    case B: return self_sum32_block<B>(blk, l, h, p, cnt);
+        MS_BW_CASES(MS_X)
+#undef MS_X
+    default: bad = true; cnt = 0; return 0;
+    }
+}
+
+}  // namespace ms
