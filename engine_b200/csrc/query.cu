@@ -466,13 +466,12 @@ __global__ void k_minmax_q(ColView c, unsigned long long *mn, unsigned long long
 // earlier blocks (scan of the per-block counts) plus the row's rank among the
 // hits of its own block, which one warp per group recomputes by decoding that
 // block of the filter and the foreign key again.  Results are compacted to
-// dense arrays in arrival order.
+// dense records (key, extent, sum, first row) in arrival order.
 __global__ void __launch_bounds__(256) k_q3_extents(GTable gt, ColView filt, ColView fk, int cmp, uint64_t c,
                                                    const uint32_t *__restrict__ bits, uint64_t lo, uint64_t span,
                                                    const uint64_t *__restrict__ blk_off,
-                                                   unsigned long long *__restrict__ cnt, uint64_t *__restrict__ o_key,
-                                                   uint64_t *__restrict__ o_ext, uint64_t *__restrict__ o_sum,
-                                                   uint64_t *__restrict__ o_row, unsigned *err) {
+                                                   unsigned long long *__restrict__ cnt,
+                                                   uint64_t *__restrict__ o, unsigned *err) {
     const unsigned lane = threadIdx.x & 31u, l = lane & 7u, q = lane >> 3;
     bool ok = true;
     for (uint64_t h = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) / 32; h <= gt.mask;
@@ -500,10 +499,10 @@ __global__ void __launch_bounds__(256) k_q3_extents(GTable gt, ColView filt, Col
         rk = __shfl_sync(0xFFFFFFFFu, rk, int((s / 16u) * 8u + unsigned(row % 8)));
         if (lane == 0) {
             const unsigned long long i = atomicAdd(cnt, 1ull);
-            o_key[i] = key;
-            o_ext[i] = blk_off[b] + rk;
-            o_sum[i] = gt.sums[h];
-            o_row[i] = row;
+            o[4 * i] = key;
+            o[4 * i + 1] = blk_off[b] + rk;
+            o[4 * i + 2] = gt.sums[h];
+            o[4 * i + 3] = row;
         }
     }
     if (!ok) atomicOr(err, kErrCorrupt);
@@ -511,6 +510,7 @@ __global__ void __launch_bounds__(256) k_q3_extents(GTable gt, ColView filt, Col
 
 bool random_access(const ColView &v) { return plain(v) || v.fmt == MS_FMT_FOR_DVBP; }
 
+constexpr uint64_t kQFirstGroups = 4096;  // group records read back with the counts
 constexpr size_t kQSmemMax = 232448;  // 227 KiB of dynamic shared memory per CTA
 
 // launch configuration of the staged kernel (consumer warps 8/16/24)
@@ -636,7 +636,7 @@ extern "C" int ms_gpu_query3(const ms_col *filter, int cmp, uint64_t c, const ms
     // The global group table starts at 2^16 slots and grows by 16x (up to
     // 2^24) when it fills, re-running the pass.
     uint64_t slots = uint64_t(1) << 16;
-    std::vector<uint64_t> k, e, s, r;
+    std::vector<uint64_t> rec;  // (key, extent, sum, first row) per group
     uint64_t ng = 0, np = 0;
     for (;;) {
         const uint64_t mark = a->used;
@@ -673,15 +673,19 @@ extern "C" int ms_gpu_query3(const ms_col *filter, int cmp, uint64_t c, const ms
             }
             MS_CUDA_TRY((scan_exclusive<uint32_t, 1>(hits, nbt, boff, tot, scr, st)));
             k_q3_extents<<<unsigned(minu(slots / 8, 4096)), 256, 0, st>>>(
-                gt, fv, kv, cmp, c, bits, lo, span, boff, cnt, out, out + slots, out + 2 * slots, out + 3 * slots,
-                a->d_err);
+                gt, fv, kv, cmp, c, bits, lo, span, boff, cnt, out, a->d_err);
             MS_CUDA_TRY(cudaGetLastError());
         }
+        // counts, error word and the first kQFirstGroups records in one
+        // read-back; more groups take a second copy
         unsigned herr = 0;
         uint64_t hc[2] = {0, 0};
+        const uint64_t first = minu(slots, kQFirstGroups);
+        rec.resize(4 * first);
         MS_CUDA_TRY(cudaMemcpyAsync(&herr, a->d_err, sizeof herr, cudaMemcpyDeviceToHost, st));
         MS_CUDA_TRY(cudaMemcpyAsync(hc, cnt, 8, cudaMemcpyDeviceToHost, st));
         MS_CUDA_TRY(cudaMemcpyAsync(hc + 1, tot, 8, cudaMemcpyDeviceToHost, st));
+        if (nbt) MS_CUDA_TRY(cudaMemcpyAsync(rec.data(), out, 32 * first, cudaMemcpyDeviceToHost, st));
         MS_CUDA_TRY(cudaStreamSynchronize(st));
         if (herr == kErrCapacity && slots < (uint64_t(1) << 24)) {
             MS_CUDA_TRY(cudaMemsetAsync(a->d_err, 0, sizeof herr, st));
@@ -693,15 +697,10 @@ extern "C" int ms_gpu_query3(const ms_col *filter, int cmp, uint64_t c, const ms
         if (rc) return rc;
         ng = hc[0];
         np = hc[1];
-        k.resize(ng);
-        e.resize(ng);
-        s.resize(ng);
-        r.resize(ng);
-        if (ng) {
-            MS_CUDA_TRY(cudaMemcpyAsync(k.data(), out, 8 * ng, cudaMemcpyDeviceToHost, st));
-            MS_CUDA_TRY(cudaMemcpyAsync(e.data(), out + slots, 8 * ng, cudaMemcpyDeviceToHost, st));
-            MS_CUDA_TRY(cudaMemcpyAsync(s.data(), out + 2 * slots, 8 * ng, cudaMemcpyDeviceToHost, st));
-            MS_CUDA_TRY(cudaMemcpyAsync(r.data(), out + 3 * slots, 8 * ng, cudaMemcpyDeviceToHost, st));
+        if (ng > first) {
+            rec.resize(4 * ng);
+            MS_CUDA_TRY(cudaMemcpyAsync(rec.data() + 4 * first, out + 4 * first, 32 * (ng - first),
+                                        cudaMemcpyDeviceToHost, st));
             MS_CUDA_TRY(cudaStreamSynchronize(st));
         }
         break;
@@ -710,14 +709,14 @@ extern "C" int ms_gpu_query3(const ms_col *filter, int cmp, uint64_t c, const ms
     // group ids follow the first occurrence: order by first row
     std::vector<uint64_t> idx(ng);
     for (uint64_t i = 0; i < ng; i++) idx[i] = i;
-    std::sort(idx.begin(), idx.end(), [&](uint64_t x, uint64_t y) { return r[x] < r[y]; });
+    std::sort(idx.begin(), idx.end(), [&](uint64_t x, uint64_t y) { return rec[4 * x + 3] < rec[4 * y + 3]; });
     *n_groups = ng;
     if (n_rows_p) *n_rows_p = np;
     if (ng > cap) return ms_fail(MS_ERR_NOMEM, "query3: more groups than the output capacity");
     for (uint64_t i = 0; i < ng; i++) {
-        if (h_keys) h_keys[i] = k[idx[i]];
-        if (h_ext) h_ext[i] = e[idx[i]];
-        if (h_sums) h_sums[i] = s[idx[i]];
+        if (h_keys) h_keys[i] = rec[4 * idx[i]];
+        if (h_ext) h_ext[i] = rec[4 * idx[i] + 1];
+        if (h_sums) h_sums[i] = rec[4 * idx[i] + 2];
     }
     return MS_OK;
 }
