@@ -10,12 +10,23 @@ larger than L2 (1.0 GB compressed), so no flush is needed between steps.
 
 value: algorithmic GB/s = (compressed bytes of x + y + 8-B result) / kernel
 time, inputs resident in HBM.  e2e: the same through the public C ABI with
-host buffers: each step copies both compressed columns (and their block
-indexes) from pinned host memory, runs the operator and reads the sum back.
+host buffers in the reference's byte layout: each step builds the block
+indexes on the host, copies both compressed columns and their indexes from
+pinned host memory, runs the operator and reads the sum back.  Rank r of N
+holds rows [r 2^28, (r+1) 2^28) of one table.
+
+Parity: the sum and count are checked on the device against torch over the
+uncompressed rows and, at N = 1, against the reference's own operators run
+over exactly the same rows on the host cores.  Further legs (each reported
+beside the headline, not as it): the learned format selector, the fused
+star query, the batched many-column execution, the codec round-trip sweep
+and a one-core CPU baseline.
 
 `--impl reference` times the reference's own CPU implementation (the
 MorphStore operators compiled from source under oracle/_ref, or the C
-restatement of them when that library is absent) on the host cores.
+restatement of them when that library is absent) on all host cores over the
+GPU arm's whole table.  `--gpus N` without a launcher starts N ranks under
+torch.distributed.run.
 """
 from __future__ import annotations
 
@@ -129,45 +140,11 @@ def _dist():
 # ---------------------------------------------------------------------------
 # reference / CPU baseline
 # ---------------------------------------------------------------------------
-def _cpu_sample_rows():
-    return 1 << 24
-
-
-_WORKER = {}
-
-
-def _cpu_init(kind):
-    """Pool initializer: the oracle / reference libraries, loaded once."""
-    import oracle
-    _WORKER["orc"] = oracle.Oracle()
-    _WORKER["ref"] = oracle.Reference(oracle.reference_path()) if kind == "reference" else None
-
-
-def _cpu_worker(args):
-    """One process: its shard (generated once per process and kept), then the
-    reference operators timed on it.  Returns (seconds, compressed bytes,
-    sum)."""
-    shard, rows, kind = args
-    import oracle
-    if "orc" not in _WORKER:
-        _cpu_init(kind)
-    orc = _WORKER["orc"]
-    key = ("data", shard, rows)
-    if key not in _WORKER:
-        _WORKER[key] = (orc.uniform_bits(SEED_X + shard, X_BITS, rows), orc.uniform_bits(SEED_Y + shard, Y_BITS, rows))
-    x, y = _WORKER[key]
-    if kind == "reference":
-        s, cnt, secs, cb = _WORKER["ref"].bench_select_project_sum(x, y, PRED)
-        return secs, cb, s
-    # port: the C restatement (decompress both columns, then select/project/sum)
-    bx, mx = orc.compress(oracle.DYNAMIC_VBP, 0, x)
-    by, my = orc.compress(oracle.DYNAMIC_VBP, 0, y)
-    t0 = time.perf_counter()
-    dx = orc.decompress(oracle.DYNAMIC_VBP, 0, bx, mx)
-    dy = orc.decompress(oracle.DYNAMIC_VBP, 0, by, my)
-    s, _ = orc.select_project_sum(oracle.CMP_LT, PRED, dx, dy)
-    secs = time.perf_counter() - t0
-    return secs, mx[1] + my[1], s
+def _config(n, world, compressed_per_gpu):
+    """The workload as both arms name it."""
+    return {"workload": WORKLOAD, "rows_per_gpu": n, "total_rows": world * n,
+            "compressed_bytes_per_gpu": int(compressed_per_gpu),
+            "parallelism": "single" if world == 1 else f"rows split across {world} ranks"}
 
 
 def _cpu_kind():
@@ -175,60 +152,73 @@ def _cpu_kind():
     return "reference" if oracle.reference_path() else "port"
 
 
-def _cpu_sample(procs, kind, rows):
-    isa = ""
-    if kind == "reference":
-        import oracle
-        isa = "avx512" if oracle.host_has_avx512() else "avx2"
-    return (f"{procs} process(es) x {rows} rows (2^24) each, same shapes and seeds scheme as the workload; "
-            f"operator time only (inputs compressed beforehand); {kind}{'/' + isa if isa else ''}")
+def _isa(kind):
+    import oracle
+    if kind != "reference":
+        return "C restatement"
+    return "reference/" + ("avx512" if oracle.host_has_avx512() else "avx2")
 
 
-def _cpu_step(pool, procs, kind, rows):
-    res = pool.map(_cpu_worker, [(i, rows, kind) for i in range(procs)])
-    secs = max(r[0] for r in res)
-    return sum(r[1] for r in res) / secs / 1e9
-
-
-def cpu_baseline(procs: int, reps: int = 1):
-    import multiprocessing as mp
+def cpu_baseline(log2_rows: int = 24, reps: int = 3):
+    """The reference's operators on one host core, on rows [0, 2^log2_rows)
+    of the benchmark's columns (operator time only, best of `reps`)."""
+    from oracle import workloads
     kind = _cpu_kind()
-    rows = _cpu_sample_rows()
-    with mp.get_context("spawn").Pool(procs, initializer=_cpu_init, initargs=(kind,)) as pool:
-        best = max(_cpu_step(pool, procs, kind, rows) for _ in range(reps))
-    return {"value": round(best, 3), "unit": "GB/s", "cores": procs, "kind": kind,
-            "sample": _cpu_sample(procs, kind, rows)}
+    rows = 1 << log2_rows
+    with workloads.ShardWorkers(rows, 1, kind) as w:
+        cb = w.prepare()
+        w.run()
+        secs = min(w.run()[0] for _ in range(reps))
+    return {"value": round(cb / secs / 1e9, 3), "unit": "GB/s", "cores": 1, "kind": kind,
+            "sample": f"rows [0, 2^{log2_rows}) of the workload's x and y, 1 process, {_isa(kind)}, operator time "
+                      f"only (inputs compressed beforehand), best of {reps}",
+            "host": workloads.host_record()}
+
+
+def reference_check(n):
+    """The reference's result over exactly the GPU's rows, on every host core:
+    (sum, count, compressed bytes)."""
+    from oracle import workloads
+    kind = _cpu_kind()
+    with workloads.ShardWorkers(n, max(1, os.cpu_count() or 1), kind) as w:
+        cb = w.prepare()
+        _, s, cnt = w.run()
+    return s, cnt, cb, kind
 
 
 def run_reference(args):
-    """The reference's own CPU operators on every host core: each step is one
-    pass over a 2^24-row sample per process (the processes and their samples
-    persist across steps)."""
-    import multiprocessing as mp
+    """The reference's own CPU operators on every host core over the GPU arm's
+    whole table (rows split into page-aligned shards, one process per core;
+    each shard generated and compressed once before timing).  A step is one
+    pass of select -> project -> sum over all rows; its time is the slowest
+    process's operator time."""
+    from oracle import workloads
     rank, world, _ = _dist()
     if rank != 0:
         return 0
+    n = 1 << args.log2_rows
+    total = world * n
     procs = max(1, os.cpu_count() or 1)
     kind = _cpu_kind()
-    rows = _cpu_sample_rows()
-    with mp.get_context("spawn").Pool(procs, initializer=_cpu_init, initargs=(kind,)) as pool:
+    with workloads.ShardWorkers(total, procs, kind) as w:
+        cb = w.prepare()
         for _ in range(max(1, args.warmup)):
-            _cpu_step(pool, procs, kind, rows)
-        vals = []
-        t0 = time.perf_counter()
+            w.run()
+        secs = []
         for _ in range(args.steps):
-            vals.append(_cpu_step(pool, procs, kind, rows))
-        wall = time.perf_counter() - t0
-    value = round(float(np.median(vals)), 3)
-    cb = cpu_baseline(1)
-    cb_all = {"value": value, "unit": "GB/s", "cores": procs, "kind": kind,
-              "sample": f"each step: {procs} processes x 2^24 rows, reference operators on the host cores"}
+            t, s, cnt = w.run()
+            secs.append(t)
+        nshards, used = len(w.shards), w.procs
+    value = round(cb * len(secs) / sum(secs) / 1e9, 3)
     line = {"metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": round(1000 * wall / max(1, args.steps), 3),
+            "warmup": args.warmup, "ms_per_step": round(1000 * statistics.mean(secs), 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-            "impl": "reference", "config": {"workload": WORKLOAD + " (CPU sample: 2^24 rows per process)",
-                                            "parallelism": f"{procs} host processes"},
-            "cpu_baseline": cb_all, "single_thread_gbs": cb["value"],
+            "impl": "reference", "config": _config(n, world, cb // world),
+            "result": {"sum": s, "count": cnt},
+            "cpu_baseline": {"value": value, "unit": "GB/s", "cores": used, "kind": kind,
+                             "sample": f"each step: all {total} rows of the workload in {nshards} page-aligned "
+                                       f"shards over {used} processes, {_isa(kind)}, operator time only",
+                             "host": workloads.host_record()},
             "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -256,8 +246,10 @@ def run_gpu(args):
     n = 1 << args.log2_rows
     xu = arena.alloc(8 * n)
     yu = arena.alloc(8 * n)
-    ms._check(lib.ms_gpu_gen_uniform_bits(SEED_X + rank, X_BITS, n, xu, sp), "gen x")
-    ms._check(lib.ms_gpu_gen_uniform_bits(SEED_Y + rank, Y_BITS, n, yu, sp), "gen y")
+    # rank r holds rows [r n, (r+1) n) of one table (the same generator as the
+    # reference arm's shards)
+    ms._check(lib.ms_gpu_gen_uniform_bits_at(SEED_X, X_BITS, rank * n, n, xu, sp), "gen x")
+    ms._check(lib.ms_gpu_gen_uniform_bits_at(SEED_Y, Y_BITS, rank * n, n, yu, sp), "gen y")
     ux = ms.MsCol(format=ms.UNCOMPR, count_values=n, size_used_byte=8 * n, size_alloc_byte=8 * n, data=xu)
     uy = ms.MsCol(format=ms.UNCOMPR, count_values=n, size_used_byte=8 * n, size_alloc_byte=8 * n, data=yu)
     xc, yc = ms.MsCol(), ms.MsCol()
@@ -310,6 +302,7 @@ def run_gpu(args):
         torch.distributed.barrier()
     per = [a.elapsed_time(b) for a, b in ev]
     total_ms = t_all0.elapsed_time(t_all1)
+    got_sum_all = got_sum
     if world > 1:
         t = torch.tensor([total_ms], device=dev)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
@@ -323,6 +316,7 @@ def run_gpu(args):
         torch.distributed.all_reduce(comb)
         ok = bool(comb[4].item() == 0 and comb[0].item() == comb[2].item() and comb[1].item() == comb[3].item())
         got_cnt = int(comb[1].item())
+        got_sum_all = int(comb[0].item()) & ((1 << 64) - 1)
     ms_per_step = total_ms / args.steps
     kern_ms = statistics.mean(per)
     value = world * algo_bytes / (ms_per_step * 1e-3) / 1e9
@@ -332,22 +326,32 @@ def run_gpu(args):
 
     peak, peak_kind = _peaks()
     achieved = algo_bytes / (kern_ms * 1e-3) / 1e9
+    parity = {"sum_ok": ok, "sum": got_sum_all, "count": got_cnt, "checked_against": "torch on the uncompressed rows"}
+    if world == 1 and not args.no_ref_check:
+        # the reference's own operators over exactly these rows, on the host cores
+        try:
+            rs, rc, rcb, rkind = reference_check(n)
+            parity.update({"vs_reference": rs == got_sum and rc == got_cnt, "reference_sum": rs, "reference_count": rc,
+                           "reference_kind": rkind, "reference_compressed_bytes": rcb,
+                           "compressed_bytes_equal": rcb == algo_bytes - 8})
+            ok = ok and parity["vs_reference"]
+        except Exception as exc:  # reported, and the run fails: parity is not optional
+            parity.update({"vs_reference": False, "reference_error": str(exc)[:300]})
+            ok = False
     line = {"metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "rows_per_gpu": n, "compressed_bytes_per_gpu": algo_bytes,
-                       "parallelism": f"shards{world} (one per rank, results combined by all_reduce)"
-                       if world > 1 else "single",
-                       "l2": "inputs (1.0 GB) larger than L2; no flush",
-                       "launch": dict(ms.get_tuning(), source="tuning.json" if tuned else "default")},
-            "parity": {"sum_ok": ok, "count": got_cnt},
+            "config": _config(n, world, algo_bytes - 8),
+            "l2": "inputs (1.0 GB per GPU) larger than L2; no flush",
+            "launch": dict(ms.get_tuning(), source="tuning.json" if tuned else "default"),
+            "parity": parity,
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                          "traffic": _traffic_per_launch(), "kernel": "k_sps_tma (sps_tma.cu)" if ms.get_tuning()["staged"] else "k_sps (ops.cu)",
                          "algorithmic_bytes_per_launch": algo_bytes},
             "clocks": clk.summary(), "e2e": e2e, "gpu_launches": args.steps}
     if args.log2_rows != 28:
-        line["config"]["note"] = "reduced size: profiling run, not the benchmark workload"
+        line["note"] = "reduced size: profiling run, not the benchmark workload"
     arena.close()
     if not args.no_selector and world == 1:
         line["learned_selector"] = selector_run(ms, args)
@@ -359,9 +363,12 @@ def run_gpu(args):
         from engine_b200 import batch_bench
         line["batched"] = batch_bench.run(4096, 10, per_column_steps=1)
         ok = ok and line["batched"]["bit_exact"]
+    if not args.no_sweep and world == 1:
+        line["codec_sweep"] = codec_sweep_run(args.log2_rows, peak)
+        ok = ok and line["codec_sweep"]["all_roundtrips_ok"]
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
-            line["cpu_baseline"] = cpu_baseline(1)
+            line["cpu_baseline"] = cpu_baseline()
         except Exception as exc:  # baseline is reported, not required
             line["cpu_baseline"] = {"error": str(exc)[:200]}
     if world > 1:
@@ -510,9 +517,102 @@ def selector_run(ms, args):
         arena.close()
 
 
+def codec_sweep_run(log2_rows, peak):
+    """The codec round-trip sweep: uncompr -> format -> uncompr over 2^log2_rows
+    values per case, for static_vbp at every bit width (uniform over that
+    width) and dynamic_vbp, delta+dvbp, for+dvbp and rle over uniform (8, 16,
+    20, 32, 64 bits), Zipf(1.2) over [0, 2^20), sorted (gaps 1 + Geom, mean 4)
+    and runs (geometric lengths, mean 32).  Inputs are generated on the device;
+    each direction is timed with CUDA events around the public morph call
+    (which includes its size read-back) and the decoded column is compared
+    with the input on the device.  Bytes per direction: 8 n + compressed
+    size.  Compressed bytes are compared with the reference's codecs by the
+    full-size tests."""
+    import torch
+
+    import engine_b200 as ms
+    from engine_b200.datagen import geom_table, zipf_table
+    n = 1 << log2_rows
+    lib = ms.lib()
+    arena = ms.Arena(24 << 30)
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+    zipf, geo = zipf_table(1.2, 1 << 20), geom_table(0.25)
+    d_zipf, d_geo = arena.alloc(zipf.nbytes), arena.alloc(geo.nbytes)
+    ms._memcpy_h2d(d_zipf, zipf)
+    ms._memcpy_h2d(d_geo, geo)
+    base = arena.used()
+    names = {1: "static_vbp", 2: "dynamic_vbp", 3: "delta+dvbp", 4: "for+dvbp", 5: "rle"}
+
+    def make(dist, seed):
+        d = arena.alloc(8 * n)
+        if dist.startswith("uniform"):
+            ms._check(lib.ms_gpu_gen_uniform_bits(seed, int(dist[7:]), n, d, sp), "gen")
+        elif dist == "zipf":
+            ms._check(lib.ms_gpu_gen_from_table(seed, d_zipf, len(zipf), n, d, sp), "gen")
+        elif dist == "sorted":
+            ms._check(lib.ms_gpu_gen_sorted_gaps(seed, d_geo, len(geo), n, d, arena.h, sp), "gen")
+        else:
+            ms._check(lib.ms_gpu_gen_runs(seed, 5, 20, n, d, arena.h, sp), "gen")
+        return ms.MsCol(format=0, count_values=n, size_used_byte=8 * n, size_alloc_byte=8 * n, data=d)
+
+    cases = [("uniform%d" % b, ms.STATIC_VBP, b) for b in range(1, 65)]
+    for dist in ("uniform8", "uniform16", "uniform20", "uniform32", "uniform64", "zipf", "sorted", "runs"):
+        for fmt in (ms.DYNAMIC_VBP, ms.DELTA_DVBP, ms.FOR_DVBP, ms.RLE):
+            cases.append((dist, fmt, 0))
+    rows = []
+    try:
+        for dist, fmt, bw in cases:
+            ms._check(lib.ms_gpu_arena_reset(arena.h), "reset")
+            arena.alloc(base)
+            u = make(dist, 0x5EED + bw)
+            best_c = best_d = None
+            for _ in range(2):  # the second pass is timed warm (first-touch of the arena pages excluded)
+                ms._check(lib.ms_gpu_arena_reset(arena.h), "reset")
+                arena.alloc(base + 8 * n)
+                c, d = ms.MsCol(), ms.MsCol()
+                torch.cuda.synchronize()
+                e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+                e0.record(stream)
+                ms._check(lib.ms_gpu_morph(C.byref(u), fmt, bw, C.byref(c), arena.h, sp), "compress")
+                e1.record(stream)
+                ms._check(lib.ms_gpu_morph(C.byref(c), ms.UNCOMPR, 0, C.byref(d), arena.h, sp), "decompress")
+                e2.record(stream)
+                torch.cuda.synchronize()
+                best_c, best_d = e0.elapsed_time(e1), e1.elapsed_time(e2)
+            ms._check(lib.ms_gpu_arena_check(arena.h, sp), "sweep kernels")
+            ok = bool(torch.equal(ms._device_view(u.data, 8 * n), ms._device_view(d.data, 8 * n)))
+            cb = int(c.size_used_byte)
+            byt = 8 * n + cb
+            rows.append([dist, names[fmt] + (f"<{bw}>" if bw else ""), cb, round(byt / best_c / 1e6, 1),
+                         round(byt / best_d / 1e6, 1), ok])
+    finally:
+        arena.close()
+
+    def frac(col, pred):
+        v = [r[col] for r in rows if pred(r)]
+        return {"min": round(min(v) / peak, 3), "median": round(statistics.median(v) / peak, 3),
+                "max": round(max(v) / peak, 3)} if v else None
+
+    by_fmt = {}
+    for f in names.values():
+        sel = (lambda r, f=f: r[1].split("<")[0] == f)
+        by_fmt[f] = {"compress_frac": frac(3, sel), "decompress_frac": frac(4, sel)}
+    return {"rows": n, "cases": len(rows), "all_roundtrips_ok": all(r[5] for r in rows),
+            "columns": ["dist", "format", "compressed_bytes", "compress_gbs", "decompress_gbs", "roundtrip_ok"],
+            "results": rows, "frac_of_peak_by_format": by_fmt, "peak_gbs": peak,
+            "bytes": "8 n + compressed bytes per direction"}
+
+
 def e2e_run(ms, lib, arena, xc, yc, sp, args, exp_sum):
-    """Per step: H2D of both compressed columns + block indexes from pinned
-    host memory, the fused operator, D2H of the 8-byte sum."""
+    """The query through the public C ABI from host buffers that hold the
+    columns in the reference's byte layout.  Per step: the block index of each
+    column is built on the host from its page headers (ms_host_build_index --
+    what a caller holding reference-layout bytes has to do), both columns and
+    their indexes are copied from pinned host memory, the fused operator runs
+    and the 8-byte sum is read back.  Timed by the wall clock around all
+    steps (host index builds overlap the previous step's copies; two index
+    buffers alternate), with one synchronisation at the end."""
     import torch
     host = {}
     for name, c in (("x", xc), ("y", yc)):
@@ -520,48 +620,49 @@ def e2e_run(ms, lib, arena, xc, yc, sp, args, exp_sum):
         hb = torch.empty(used, dtype=torch.uint8, pin_memory=True)
         hb.copy_(ms._device_view(c.data, used).cpu())
         nb = int(c.n_index)
-        hi = torch.empty(8 * nb, dtype=torch.uint8, pin_memory=True)
-        idx = np.zeros(nb + 1, dtype=np.uint64)
-        hnp = hb.numpy()
-        ms._check(lib.ms_host_build_index(int(c.format), hnp.ctypes.data, int(c.size_compr_byte),
-                                          nb * 512, idx.ctypes.data, None), "host index")
-        hi.copy_(torch.from_numpy(idx[:nb].view(np.uint8)))
+        hidx = [torch.empty(8 * nb + 8, dtype=torch.uint8, pin_memory=True) for _ in range(2)]
         dbuf = arena.alloc(used + 64)
         didx = arena.alloc(8 * nb + 8)
         desc = ms.MsCol(format=c.format, bw=c.bw, count_values=c.count_values, size_used_byte=used,
                         size_compr_byte=c.size_compr_byte, size_alloc_byte=used + 64, data=dbuf, index=didx,
                         n_index=nb)
-        host[name] = (hb, hi, dbuf, didx, desc)
+        host[name] = (hb, hidx, dbuf, didx, desc, nb)
     d_sum = arena.alloc(8)
     d_err = arena.alloc(8)
     h_sum = torch.empty(8, dtype=torch.uint8, pin_memory=True)
     stream = torch.cuda.current_stream()
-    h2d = sum(h[0].numel() + h[1].numel() for h in host.values())
     algo = int(xc.size_used_byte) + int(yc.size_used_byte) + 8
+    done = [torch.cuda.Event(), torch.cuda.Event()]
 
-    def step():
-        for hb, hi, dbuf, didx, desc in host.values():
+    def step(i):
+        j = i & 1
+        done[j].synchronize()  # the copies that last read index buffer j have finished
+        for hb, hidx, dbuf, didx, desc, nb in host.values():
+            ms._check(lib.ms_host_build_index(int(desc.format), hb.data_ptr(), int(desc.size_compr_byte), nb * 512,
+                                              hidx[j].data_ptr(), None), "host index")
             ms._device_view(dbuf, hb.numel()).copy_(hb, non_blocking=True)
-            ms._device_view(didx, hi.numel()).copy_(hi, non_blocking=True)
+            ms._device_view(didx, 8 * nb).copy_(hidx[j][: 8 * nb], non_blocking=True)
+        done[j].record(stream)
         ms._check(lib.ms_gpu_select_project_sum_async(C.byref(host["x"][4]), ms.less, PRED, C.byref(host["y"][4]),
                                                       d_sum, None, d_err, sp), "sps e2e")
         h_sum.copy_(ms._device_view(d_sum, 8), non_blocking=True)
 
-    for _ in range(2):
-        step()
+    for i in range(2):
+        step(i)
     torch.cuda.synchronize()
     ok = int(h_sum.numpy().view(np.uint64)[0]) == exp_sum
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     k = max(1, min(args.steps, 20))
-    e0.record(stream)
-    for _ in range(k):
-        step()
-    e1.record(stream)
+    h2d = sum(h[0].numel() + 8 * h[5] for h in host.values())
+    t0 = time.perf_counter()
+    for i in range(k):
+        step(i)
     torch.cuda.synchronize()
-    ms_step = e0.elapsed_time(e1) / k
+    ms_step = 1000 * (time.perf_counter() - t0) / k
+    ok = ok and int(h_sum.numpy().view(np.uint64)[0]) == exp_sum
     return {"value": round(algo / (ms_step * 1e-3) / 1e9, 2), "unit": "GB/s", "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": 8, "ms_per_step": round(ms_step, 3), "sum_ok": ok,
-            "path": "ms_gpu_select_project_sum_async via ctypes, pinned host buffers"}
+            "path": "host page walk (ms_host_build_index) + H2D of reference-layout bytes and index from pinned "
+                    "memory + ms_gpu_select_project_sum_async + D2H of the sum, via ctypes; wall clock"}
 
 
 def main():
@@ -579,10 +680,31 @@ def main():
     ap.add_argument("--sel-steps", type=int, default=2000, help="Adam steps")
     ap.add_argument("--no-star", action="store_true", help="skip the fused star-query leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched many-column leg")
+    ap.add_argument("--no-sweep", action="store_true", help="skip the codec round-trip sweep leg")
+    ap.add_argument("--no-ref-check", action="store_true",
+                    help="skip the comparison with the reference's result over the same rows")
     args = ap.parse_args()
+    world = os.environ.get("WORLD_SIZE")
+    if args.gpus > 1 and world is None:
+        return _launch_ranks(args.gpus)
+    if world is not None and int(world) != args.gpus:
+        print(f"bench.py: --gpus {args.gpus} but WORLD_SIZE={world}", file=sys.stderr)
+        return 2
     if args.impl == "reference":
         return run_reference(args)
     return run_gpu(args)
+
+
+def _launch_ranks(n):
+    """`--gpus N` without a launcher: start N ranks (one per GPU) under
+    torch.distributed.run on 127.0.0.1 and return their status."""
+    import socket
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr=127.0.0.1", f"--master-port={port}", os.path.abspath(__file__), *sys.argv[1:]]
+    return subprocess.run(cmd).returncode
 
 
 if __name__ == "__main__":

@@ -101,6 +101,7 @@ _sig = {
     "ms_gpu_get_query_tuning": (C.c_int, [_P(MsTuning)]),
     "ms_gpu_get_tuning": (C.c_int, [_P(MsTuning)]),
     "ms_gpu_gen_uniform_bits": (C.c_int, [_U64, C.c_uint, _U64, _V, _V]),
+    "ms_gpu_gen_uniform_bits_at": (C.c_int, [_U64, C.c_uint, _U64, _U64, _V, _V]),
     "ms_gpu_gen_from_table": (C.c_int, [_U64, _V, _U64, _U64, _V, _V]),
     "ms_gpu_gen_sorted_gaps": (C.c_int, [_U64, _V, _U64, _U64, _V, _V, _V]),
     "ms_gpu_gen_runs": (C.c_int, [_U64, C.c_uint, C.c_uint, _U64, _V, _V, _V]),

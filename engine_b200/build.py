@@ -49,6 +49,7 @@ def build(verbose: bool = False) -> str:
         cmd = [NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB, *objs]
         subprocess.run(cmd, check=True)
     _build_examples()
+    _build_reference_sources()
     return LIB
 
 
@@ -68,6 +69,58 @@ def _build_examples() -> None:
                "-I", os.path.join(HERE, "include"), srcp, "-o", binp, "-L", HERE, "-lms_gpu",
                "-Wl,-rpath,$ORIGIN/../.."]
         subprocess.run(cmd, check=True)
+
+
+# The reference's own example query and operator known-answer tests, compiled
+# against the reference's headers with the processing style changed to
+# gpu_b200 and ve_gpu_b200.h put in front (-include).  The only edit to each
+# source is the style token: `using ve = scalar<v64<uint64_t> >;` in the
+# example, every `scalar<v64<uint64_t>>` in the tests.  The edited text is
+# piped to g++ and never written out; only the binaries are kept (bin/ref_*).
+# Built where the reference tree is present (MS_REFERENCE_DIR); the binaries
+# travel with the library.
+REFERENCE_SOURCES = [
+    ("select_sum_query", "src/examples/select_sum_query.cpp", "using ve = scalar<v64<uint64_t> >;",
+     "using ve = gpu_b200<v512<uint64_t> >;"),
+] + [(f"kat_{n}", f"test/core/operators/{n}.cpp", "scalar<v64<uint64_t>>", "gpu_b200<v512<uint64_t>>")
+     for n in ("select_test", "project_test", "agg_sum_whole_column_test", "agg_sum_group_based_test",
+               "group_unary_test", "group_binary_test", "intersect_test")]
+
+
+def _build_reference_sources() -> None:
+    ref = os.environ.get("MS_REFERENCE_DIR")
+    if not ref or not os.path.isdir(os.path.join(ref, "include", "core")):
+        return
+    root = os.path.dirname(HERE)
+    gen = os.path.join(root, "oracle", "_ref", "gen")
+    if not os.path.exists(os.path.join(gen, "core", "morphing", "vbp_routines.h")):
+        subprocess.run(["make", "-s", "-C", os.path.join(root, "oracle"), f"MS_REFERENCE_DIR={ref}",
+                        os.path.join(gen, "core", "morphing", "vbp_routines.h")], check=True)
+    out = os.path.join(HERE, "examples", "bin")
+    os.makedirs(out, exist_ok=True)
+    hdr = os.path.join(HERE, "include", "morphstore_b200", "ve_gpu_b200.h")
+    flags = ["-std=c++14", "-O2", "-DMSV_NO_SELFMANAGED_MEMORY", "-DMSV_NO_LOG", "-DMSV_MEMORY_MANAGER_ALIGNMENT_BYTE=64",
+             "-Wno-ignored-attributes", "-I", gen, "-I", os.path.join(ref, "include"),
+             "-I", os.path.join(root, "include"), "-I", os.path.join(HERE, "include")]
+
+    def one(item):
+        name, rel, old, new = item
+        src = os.path.join(ref, rel)
+        binp = os.path.join(out, "ref_" + name)
+        deps = [src, hdr, LIB, os.path.join(root, "include", "ms_gpu.h")]
+        if os.path.exists(binp) and os.path.getmtime(binp) > max(os.path.getmtime(d) for d in deps):
+            return
+        text = open(src).read()
+        if text.count(old) < 1 or (name == "select_sum_query" and text.count(old) != 1):
+            raise RuntimeError(f"{rel}: processing-style token not found as expected")
+        cmd = ["g++", *flags, "-I", os.path.dirname(src), "-include", hdr, "-x", "c++", "-", "-o", binp,
+               "-L", HERE, "-lms_gpu", "-Wl,-rpath,$ORIGIN/../.."]
+        r = subprocess.run(cmd, input=text.replace(old, new), capture_output=True, text=True)
+        if r.returncode:
+            raise RuntimeError(f"g++ failed for {rel}:\n{r.stderr[-4000:]}")
+
+    with cf.ThreadPoolExecutor(max_workers=8) as ex:
+        list(ex.map(one, REFERENCE_SOURCES))
 
 
 if __name__ == "__main__":

@@ -441,9 +441,10 @@ __global__ void __launch_bounds__(32 * W, 1)
         __syncwarp();
         consumed++;
     }
-    // a failed wait leaves copies in flight: wait for them (bounded) before leaving
+    // a failed wait leaves copies in flight, the one it gave up on included:
+    // wait for them (bounded) before leaving
     if (!ok)
-        for (unsigned t = consumed + 1; t < issued; t++) mbar_wait(bar + t % S, (t / S) & 1u);
+        for (unsigned t = consumed; t < issued; t++) mbar_wait(bar + t % S, (t / S) & 1u);
     if (!ok && lane == 0) atomicOr(err, kErrTimeout);
     if (bad && lane == 0) atomicOr(err, kErrCorrupt);
 }

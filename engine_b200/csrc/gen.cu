@@ -13,9 +13,10 @@ __device__ __forceinline__ uint64_t mix64(uint64_t seed, uint64_t i) {
     return z ^ (z >> 31);
 }
 
-__global__ void k_uniform_bits(uint64_t seed, unsigned bits, uint64_t n, uint64_t *__restrict__ out) {
+__global__ void k_uniform_bits(uint64_t seed, unsigned bits, uint64_t row0, uint64_t n,
+                               uint64_t *__restrict__ out) {
     for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
-        const uint64_t z = mix64(seed, i);
+        const uint64_t z = mix64(seed, row0 + i);
         out[i] = bits >= 64 ? z : (bits == 0 ? 0 : z >> (64 - bits));
     }
 }
@@ -38,12 +39,17 @@ __global__ void k_from_table(uint64_t seed, const uint64_t *__restrict__ table, 
 }  // namespace
 }  // namespace ms
 
-extern "C" int ms_gpu_gen_uniform_bits(uint64_t seed, unsigned bits, uint64_t n, uint64_t *d_out, void *stream) {
+extern "C" int ms_gpu_gen_uniform_bits_at(uint64_t seed, unsigned bits, uint64_t row0, uint64_t n, uint64_t *d_out,
+                                          void *stream) {
     if (!d_out && n) return ms_fail(MS_ERR_INVALID, "gen_uniform_bits: null output");
     if (!n) return MS_OK;
-    ms::k_uniform_bits<<<ms::persistent_grid(256, 8), 256, 0, (cudaStream_t)stream>>>(seed, bits, n, d_out);
+    ms::k_uniform_bits<<<ms::persistent_grid(256, 8), 256, 0, (cudaStream_t)stream>>>(seed, bits, row0, n, d_out);
     MS_CUDA_TRY(cudaGetLastError());
     return MS_OK;
+}
+
+extern "C" int ms_gpu_gen_uniform_bits(uint64_t seed, unsigned bits, uint64_t n, uint64_t *d_out, void *stream) {
+    return ms_gpu_gen_uniform_bits_at(seed, bits, 0, n, d_out, stream);
 }
 
 extern "C" int ms_gpu_gen_from_table(uint64_t seed, const uint64_t *d_table, uint64_t n_table, uint64_t n,

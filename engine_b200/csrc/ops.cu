@@ -292,12 +292,17 @@ extern "C" int ms_gpu_agg_sum(const ms_col *in, uint64_t *d_sum, ms_arena *a, vo
 extern "C" int ms_gpu_select(int cmp, uint64_t val, const ms_col *in, int out_format, unsigned out_bw, ms_col *out,
                              ms_arena *a, void *stream) {
     if (!in || !out || !a) return ms_fail(MS_ERR_INVALID, "select: null argument");
+    const bool all_unsigned = (cmp & MS_CMP_UNSIGNED) != 0;
+    cmp &= ~MS_CMP_UNSIGNED;
     if (cmp < MS_CMP_EQ || cmp > MS_CMP_GE) return ms_fail(MS_ERR_INVALID, "select: unknown comparison");
     if (in->format == MS_FMT_RLE) return ms_fail(MS_ERR_UNSUPPORTED, "select: rle_f input has no sequential reader");
     cudaStream_t st = (cudaStream_t)stream;
     ColView x;
     int rc = prepare_view(in, a, st, &x);
     if (rc) return rc;
+    // the scalar style compares every row unsigned: its "remainder" is the
+    // whole column, and all hits are written as remainder rows
+    if (all_unsigned) x.sfrom = 0;
     uint64_t *pos, cnt, nscal;
     rc = select_positions(x, nullptr, cmp, val, a, st, &pos, nullptr, &cnt, &nscal);
     if (rc) return rc;
@@ -393,7 +398,7 @@ extern "C" int ms_gpu_select_project_sum_async(const ms_col *xc, int cmp, uint64
 // plugin host), and paths where cudaMalloc / cudaFree are forbidden because
 // they synchronise the device.  For them this entry point takes the caller's
 // input and output buffers and keeps its own scratch (per-block hit counts,
-// block offsets, scan partials, two counters) in one file-scope device
+// block offsets, scan partials, the scalar-remainder hit counter) in one file-scope device
 // array, kNoAllocScratchBytes large, which every GPU that loads the library
 // holds until the process exits.  Inputs are limited to kNoAllocMaxRows rows
 // so that the scratch fits.
@@ -404,7 +409,11 @@ extern "C" int ms_gpu_select_project_sum_async(const ms_col *xc, int cmp, uint64
 // therefore happen before any stream capture.  Every call shares the one
 // array and it keeps the last call's contents, so calls that overlap on the
 // GPU (concurrent streams, other threads) race; the counters that must start
-// at zero are cleared at the start of every call.
+// at zero are cleared at the start of every call.  The looked-up address is
+// kept for the life of the process, so the entry point must not be used on a
+// device after cudaDeviceReset (or after the primary context was otherwise
+// destroyed and re-created).  Kernel errors (a corrupt header or bit width)
+// go to the caller's d_err word, which is therefore required.
 // ---------------------------------------------------------------------------
 namespace {
 
@@ -415,7 +424,7 @@ constexpr uint64_t kNoAllocCountsBytes = round256(4 * kNoAllocMaxBlocks);
 constexpr uint64_t kNoAllocOffsetsBytes = round256(8 * kNoAllocMaxBlocks);
 constexpr uint64_t kNoAllocScanWords = 2 * ((kNoAllocMaxBlocks + kScanTile - 1) / kScanTile) + 2 * 1 + 1;
 constexpr uint64_t kNoAllocScanBytes = round256(8 * kNoAllocScanWords);
-constexpr uint64_t kNoAllocWordsBytes = 256;  // scalar-hit counter, error word
+constexpr uint64_t kNoAllocWordsBytes = 256;  // scalar-hit counter
 constexpr uint64_t kNoAllocScratchBytes =
     kNoAllocCountsBytes + kNoAllocOffsetsBytes + kNoAllocScanBytes + kNoAllocWordsBytes;
 
@@ -445,8 +454,8 @@ extern "C" uint64_t ms_gpu_select_noalloc_max_rows(void) { return kNoAllocMaxRow
 
 extern "C" int ms_gpu_select_noalloc(int cmp, uint64_t val, const ms_col *in, uint64_t *d_out_pos,
                                      uint64_t out_capacity, uint64_t *d_out_count, unsigned *d_err, void *stream) {
-    if (!in || !d_out_count || (!d_out_pos && in->count_values))
-        return ms_fail(MS_ERR_INVALID, "select_noalloc: null argument");
+    if (!in || !d_out_count || !d_err || (!d_out_pos && in->count_values))
+        return ms_fail(MS_ERR_INVALID, "select_noalloc: null argument (d_out_count and d_err are required)");
     if (cmp < MS_CMP_EQ || cmp > MS_CMP_GE) return ms_fail(MS_ERR_INVALID, "select_noalloc: unknown comparison");
     int rc = check_col(in, false);
     if (rc) return rc;
@@ -468,14 +477,13 @@ extern "C" int ms_gpu_select_noalloc(int cmp, uint64_t val, const ms_col *in, ui
     uint64_t *scan_scr = reinterpret_cast<uint64_t *>(scr + kNoAllocCountsBytes + kNoAllocOffsetsBytes);
     unsigned long long *scalar_hits =
         reinterpret_cast<unsigned long long *>(scr + kNoAllocCountsBytes + kNoAllocOffsetsBytes + kNoAllocScanBytes);
-    unsigned *own_err = reinterpret_cast<unsigned *>(scalar_hits + 1);
-    unsigned *err = d_err ? d_err : own_err;
+    unsigned *err = d_err;
     cudaStream_t st = (cudaStream_t)stream;
     ColView x;
     rc = prepare_view(in, nullptr, st, &x);
     if (rc) return rc;
     MS_CUDA_TRY(cudaMemsetAsync(scalar_hits, 0, kNoAllocWordsBytes, st));
-    if (d_err) MS_CUDA_TRY(cudaMemsetAsync(d_err, 0, sizeof(unsigned), st));
+    MS_CUDA_TRY(cudaMemsetAsync(d_err, 0, sizeof(unsigned), st));
     const uint64_t nbt = x.nblocks_total();
     if (nbt == 0) {
         MS_CUDA_TRY(cudaMemsetAsync(d_out_count, 0, 8, st));

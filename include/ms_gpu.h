@@ -60,6 +60,10 @@ enum {
  * unsigned, as in the reference's AVX-512 build (compare_avx512.h:35-111,
  * compare_scalar.h:17-77); both agree for values below 2^63. */
 enum { MS_CMP_EQ = 0, MS_CMP_LT = 1, MS_CMP_LE = 2, MS_CMP_GT = 3, MS_CMP_GE = 4 };
+/* OR-ed into ms_gpu_select's `cmp`: compare every row as unsigned, as the
+ * scalar processing style's select_t<std::less, scalar<v64<uint64_t>>, ...>
+ * does (scalar/select_uncompr.h:39-77, compare_scalar.h:37). */
+enum { MS_CMP_UNSIGNED = 16 };
 
 /* Device-resident column descriptor (column<F> metadata, column.h:133-144).
  * `index` is an optional device array built by ms_gpu_build_index (or by the
@@ -228,14 +232,18 @@ int ms_gpu_agg_sum_grouped(const ms_col *gr, const ms_col *data, uint64_t n_grou
  * synchronise the device.  The caller passes the input column and the output
  * buffers: d_out_pos (capacity out_capacity >= count_values; uncompressed
  * ascending positions) and d_out_count (the hit count, device memory);
- * d_err (optional, device) receives kernel error bits.  Nothing is allocated:
+ * d_err (required, device) is cleared and then receives kernel error bits
+ * (1 = corrupt header or bit width), which the caller reads after the stream
+ * has run; the call itself only reports argument errors.  Nothing is allocated:
  * scratch lives in a 2 MiB file-scope device array that every GPU loading the
  * library keeps until exit, so inputs are limited to
  * ms_gpu_select_noalloc_max_rows() = 2^26 rows; longer inputs, delta_f/rle_f
  * inputs and dynamic_vbp/for_f inputs without a block index are rejected.
  * The first call on a device looks up the array's device address, so make it
- * before any stream capture.  All calls share the array and it keeps the last
- * call's contents: calls that overlap on the GPU race.  Asynchronous. */
+ * before any stream capture; the address is kept for the life of the
+ * process, so do not call it on a device after cudaDeviceReset.  All calls
+ * share the array and it keeps the last call's contents: calls that overlap
+ * on the GPU race.  Asynchronous. */
 int ms_gpu_select_noalloc(int cmp, uint64_t val, const ms_col *in, uint64_t *d_out_pos,
                           uint64_t out_capacity, uint64_t *d_out_count, unsigned *d_err, void *stream);
 uint64_t ms_gpu_select_noalloc_max_rows(void);
@@ -335,6 +343,9 @@ int ms_gpu_mlp_load(ms_mlp *m, const void *h_state);
 
 /* ---- synthetic data (device-side, counter-based splitmix64) -------------- */
 int ms_gpu_gen_uniform_bits(uint64_t seed, unsigned bits, uint64_t n, uint64_t *d_out, void *stream);
+/* rows [row0, row0 + n) of the same column: one rank's shard of a table */
+int ms_gpu_gen_uniform_bits_at(uint64_t seed, unsigned bits, uint64_t row0, uint64_t n, uint64_t *d_out,
+                               void *stream);
 int ms_gpu_gen_from_table(uint64_t seed, const uint64_t *d_table, uint64_t n_table, uint64_t n,
                           uint64_t *d_out, void *stream);
 /* sorted ascending: prefix sums of 1 + (draw from the gap table) */

@@ -95,6 +95,7 @@ class Oracle:
         L.orc_mix64.restype = C.c_uint64
         L.orc_mix64.argtypes = [C.c_uint64, C.c_uint64]
         L.orc_gen_uniform_bits.argtypes = [C.c_uint64, C.c_uint, C.c_uint64, U64P]
+        L.orc_gen_uniform_bits_at.argtypes = [C.c_uint64, C.c_uint, C.c_uint64, C.c_uint64, U64P]
         L.orc_cdf_table_zipf.argtypes = [C.c_double, C.c_uint64, U64P]
         L.orc_cdf_table_geom.restype = C.c_uint64
         L.orc_cdf_table_geom.argtypes = [C.c_double, C.c_uint64, U64P]
@@ -223,9 +224,10 @@ class Oracle:
         return out[:n_groups]
 
     # --- generators -----------------------------------------------------------
-    def uniform_bits(self, seed, bits, n):
+    def uniform_bits(self, seed, bits, n, row0=0):
+        """Rows [row0, row0 + n) of the seeded uniform column."""
         out = np.empty(n, dtype=np.uint64)
-        self.lib.orc_gen_uniform_bits(seed, bits, n, out.ctypes.data_as(U64P))
+        self.lib.orc_gen_uniform_bits_at(seed, bits, row0, n, out.ctypes.data_as(U64P))
         return out
 
     def zipf_table(self, s, n_vals):
@@ -295,6 +297,11 @@ class Reference:
         L.ref_intersect_scalar.argtypes = [U64P, C.c_uint64, U64P, C.c_uint64, U64P]
         L.ref_group.argtypes = [C.c_int, U8P, M, C.c_int, U8P, C.c_uint64, M, C.c_int, U8P, C.c_uint64, M]
         L.ref_agg_sum_grouped.argtypes = [U64P, U64P, C.c_uint64, C.c_uint64, U64P]
+        L.ref_sps_prepare.restype = C.c_void_p
+        L.ref_sps_prepare.argtypes = [U64P, U64P, C.c_uint64, U64P]
+        L.ref_sps_run.restype = C.c_uint64
+        L.ref_sps_run.argtypes = [C.c_void_p, C.c_uint64, C.POINTER(C.c_double), U64P]
+        L.ref_sps_free.argtypes = [C.c_void_p]
         L.ref_bench_select_project_sum.restype = C.c_uint64
         L.ref_bench_select_project_sum.argtypes = [U64P, U64P, C.c_uint64, C.c_uint64, C.POINTER(C.c_double),
                                                    U64P, U64P]
@@ -427,6 +434,26 @@ class Reference:
         out = np.zeros(max(n_groups, 1), dtype=np.uint64)
         self.lib.ref_agg_sum_grouped(gp, dp, len(d), n_groups, out.ctypes.data_as(U64P))
         return out[:n_groups]
+
+    def sps_prepare(self, x, y):
+        """Compress x and y (dynamic_vbp) with the reference and keep them:
+        (handle, compressed bytes)."""
+        x, xp = _u64(x)
+        y, yp = _u64(y)
+        cb = C.c_uint64(0)
+        h = self.lib.ref_sps_prepare(xp, yp, len(x), C.byref(cb))
+        return h, int(cb.value)
+
+    def sps_run(self, handle, c):
+        """select(x < c) -> project(y) -> agg_sum on a prepared pair:
+        (sum, count, operator seconds)."""
+        secs = C.c_double(0)
+        cnt = C.c_uint64(0)
+        s = self.lib.ref_sps_run(handle, c, C.byref(secs), C.byref(cnt))
+        return int(s), int(cnt.value), float(secs.value)
+
+    def sps_free(self, handle):
+        self.lib.ref_sps_free(handle)
 
     def bench_select_project_sum(self, x, y, c):
         x, xp = _u64(x)

@@ -612,8 +612,13 @@ uint64_t orc_mix64(uint64_t seed, uint64_t i) {
 }
 
 void orc_gen_uniform_bits(uint64_t seed, unsigned bits, uint64_t n, uint64_t *out) {
+    orc_gen_uniform_bits_at(seed, bits, 0, n, out);
+}
+
+/* rows [row0, row0 + n) of the same stream: a shard of a longer column */
+void orc_gen_uniform_bits_at(uint64_t seed, unsigned bits, uint64_t row0, uint64_t n, uint64_t *out) {
     for (uint64_t i = 0; i < n; i++) {
-        uint64_t z = orc_mix64(seed, i);
+        uint64_t z = orc_mix64(seed, row0 + i);
         out[i] = bits >= 64 ? z : (bits == 0 ? 0 : z >> (64 - bits));
     }
 }

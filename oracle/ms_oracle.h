@@ -94,6 +94,7 @@ void orc_agg_sum_grouped(const uint64_t *gr, const uint64_t *data, uint64_t n,
 /* ---- seeded generators (counter-based splitmix64) ----------------------- */
 uint64_t orc_mix64(uint64_t seed, uint64_t i);
 void orc_gen_uniform_bits(uint64_t seed, unsigned bits, uint64_t n, uint64_t *out);
+void orc_gen_uniform_bits_at(uint64_t seed, unsigned bits, uint64_t row0, uint64_t n, uint64_t *out);
 void orc_cdf_table_zipf(double s, uint64_t n_vals, uint64_t *table);
 uint64_t orc_cdf_table_geom(double p, uint64_t max_len, uint64_t *table);
 void orc_gen_from_table(uint64_t seed, const uint64_t *table, uint64_t n_tab,

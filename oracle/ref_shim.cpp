@@ -425,6 +425,50 @@ uint64_t ref_bench_select_project_sum(const uint64_t *x, const uint64_t *y, uint
     return sum;
 }
 
+
+// The same query split into preparation and timed runs, so that a process
+// which runs it step after step compresses its rows once: ref_sps_prepare
+// compresses x and y (dynamic_vbp, as the GPU path stores them) and keeps
+// them; ref_sps_run times select(x < c) -> morph(y) -> project -> agg_sum on
+// them (the operators of select_sum_query.cpp:77-97) and returns the sum.
+struct ref_sps {
+    const column<dv> *x, *y;
+};
+
+void *ref_sps_prepare(const uint64_t *x, const uint64_t *y, uint64_t n, uint64_t *compr_bytes) {
+    const column<uf> *xu = make_ucol(x, n);
+    const column<uf> *yu = make_ucol(y, n);
+    auto *h = new ref_sps{morph<ve, dv>(xu), morph<ve, dv>(yu)};
+    delete xu;
+    delete yu;
+    *compr_bytes = h->x->get_size_used_byte() + h->y->get_size_used_byte();
+    return h;
+}
+
+uint64_t ref_sps_run(void *handle, uint64_t c, double *secs, uint64_t *count) {
+    const ref_sps *h = static_cast<const ref_sps *>(handle);
+    auto t0 = std::chrono::steady_clock::now();
+    const column<uf> *pos = my_select_wit_t<vectorlib::less, ve, uf, dv>::apply(h->x, c);
+    const column<uf> *yd = morph<ve, uf>(h->y);
+    const column<uf> *pr = my_project_wit_t<ve, uf, uf, uf>::apply(yd, pos);
+    const column<uf> *s = agg_sum<ve, uf>(pr);
+    auto t1 = std::chrono::steady_clock::now();
+    *secs = std::chrono::duration<double>(t1 - t0).count();
+    const uint64_t sum = *(const uint64_t *)s->get_data();
+    *count = pos->get_count_values();
+    delete pos;
+    delete yd;
+    delete pr;
+    delete s;
+    return sum;
+}
+
+void ref_sps_free(void *handle) {
+    ref_sps *h = static_cast<ref_sps *>(handle);
+    delete h->x;
+    delete h->y;
+    delete h;
+}
 #endif
 
 #if defined(PART_JOIN)
