@@ -225,111 +225,243 @@ __global__ void __launch_bounds__(256) k_decode_all(ColView c, uint64_t *__restr
 }
 
 // --- rle ----------------------------------------------------------------------
-constexpr unsigned kRleTile = 4096;
+// Encoder: one pass over the input in tiles of kRleTile rows, tiles taken in
+// order from a ticket counter.  A row starts a run (a "head") when it differs
+// from the row before (rle.h:63-150: maximal runs).  Each tile needs the
+// number of runs before it (its first head's run index) and the row of the
+// last head before it (where the run its first head ends began): both come
+// from a decoupled look-back over the tiles before it (every tile publishes
+// its own run count and last head, then -- once known -- the inclusive
+// values).  Every head writes its run's value and the length of the run
+// before it; the last tile writes the length of the final run.  So the input
+// is read once and each pair written once (8 B/row + 16 B/run).
+constexpr unsigned kRleThreads = 256;
+constexpr unsigned kRleRowsPerThread = 8;
+constexpr unsigned kRleTile = kRleThreads * kRleRowsPerThread;
+constexpr uint64_t kRleNone = ~uint64_t(0);
+enum : unsigned { kRleFlagAgg = 1, kRleFlagInc = 2 };
 
-__device__ __forceinline__ bool rle_head(const uint64_t *in, uint64_t i) { return i == 0 || in[i] != in[i - 1]; }
+struct RleTileState {
+    unsigned flag;
+    unsigned pad;
+    uint64_t agg_runs, agg_last;  // this tile's runs and last head (kRleNone: none)
+    uint64_t inc_runs, inc_last;  // the same over tiles [0, this tile]
+};
 
-__global__ void __launch_bounds__(256) k_rle_count(const uint64_t *__restrict__ in, uint64_t n,
-                                                  uint32_t *__restrict__ tile_counts) {
-    __shared__ unsigned cnt;
-    if (threadIdx.x == 0) cnt = 0;
+__global__ void __launch_bounds__(kRleThreads) k_rle_encode(const uint64_t *__restrict__ in, uint64_t n,
+                                                           RleTileState *state, unsigned *ticket,
+                                                           uint64_t *__restrict__ out, uint64_t *__restrict__ d_runs,
+                                                           unsigned *err) {
+    __shared__ uint64_t s_tile;
+    __shared__ unsigned s_wcnt[kRleThreads / 32];
+    __shared__ uint64_t s_wlast[kRleThreads / 32];
+    __shared__ uint64_t s_excl_runs, s_excl_last;
+    const unsigned lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+    if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
     __syncthreads();
-    const uint64_t base = uint64_t(blockIdx.x) * kRleTile;
-    unsigned c = 0;
-    for (unsigned i = threadIdx.x; i < kRleTile; i += blockDim.x) {
-        const uint64_t r = base + i;
-        if (r < n && rle_head(in, r)) c++;
-    }
-    c = __reduce_add_sync(0xFFFFFFFFu, c);
-    if ((threadIdx.x & 31u) == 0) atomicAdd(&cnt, c);
-    __syncthreads();
-    if (threadIdx.x == 0) tile_counts[blockIdx.x] = cnt;
-}
-
-// Writes run starts in order: thread i of the tile handles rows base + 16*i..+15.
-__global__ void __launch_bounds__(256) k_rle_starts(const uint64_t *__restrict__ in, uint64_t n,
-                                                   const uint64_t *__restrict__ tile_off,
-                                                   uint64_t *__restrict__ starts) {
-    __shared__ unsigned warp_tot[8];
-    const uint64_t base = uint64_t(blockIdx.x) * kRleTile + threadIdx.x * 16u;
+    const uint64_t tile = s_tile;
+    const uint64_t ntiles = (n + kRleTile - 1) / kRleTile;
+    if (tile >= ntiles) return;
+    // this thread's rows and their heads
+    const uint64_t r0 = tile * kRleTile + uint64_t(threadIdx.x) * kRleRowsPerThread;
+    uint64_t v[kRleRowsPerThread];
+    uint64_t prev = r0 > 0 && r0 <= n ? __ldg(in + r0 - 1) : 0;
     unsigned m = 0;
 #pragma unroll
-    for (int k = 0; k < 16; k++) {
-        const uint64_t r = base + k;
-        if (r < n && rle_head(in, r)) m |= 1u << k;
+    for (unsigned k = 0; k < kRleRowsPerThread; k++) {
+        const uint64_t r = r0 + k;
+        v[k] = r < n ? __ldg(in + r) : 0;
+        if (r < n && (r == 0 || v[k] != prev)) m |= 1u << k;
+        prev = v[k];
     }
-    unsigned c = __popc(m), incl = c;
-    const unsigned lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+    const unsigned c = __popc(m);
+    // last head of this thread as row + 1 (0: none); rows grow with the thread
+    const uint64_t my_last = m ? r0 + (31 - __clz(m)) + 1 : 0;
+    // block-wide exclusive count scan and exclusive "last head before me"
+    unsigned incl = c;
+    uint64_t lmax = my_last;
 #pragma unroll
-    for (int s = 1; s < 32; s <<= 1) {
-        unsigned t = __shfl_up_sync(0xFFFFFFFFu, incl, s);
-        if (lane >= unsigned(s)) incl += t;
+    for (int d = 1; d < 32; d <<= 1) {
+        const unsigned t = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+        const uint64_t tl = __shfl_up_sync(0xFFFFFFFFu, lmax, d);
+        if (int(lane) >= d) {
+            incl += t;
+            lmax = maxu(lmax, tl);
+        }
     }
-    if (lane == 31) warp_tot[wid] = incl;
+    if (lane == 31) {
+        s_wcnt[wid] = incl;
+        s_wlast[wid] = lmax;
+    }
     __syncthreads();
     unsigned wpre = 0;
-    for (unsigned w = 0; w < wid; w++) wpre += warp_tot[w];
-    uint64_t pos = tile_off[blockIdx.x] + wpre + incl - c;
-    while (m) {
-        const int k = __ffs(m) - 1;
-        starts[pos++] = base + k;
-        m &= m - 1;
+    uint64_t wlast = 0;
+    for (unsigned w = 0; w < wid; w++) {
+        wpre += s_wcnt[w];
+        wlast = maxu(wlast, s_wlast[w]);
     }
-}
-
-__global__ void k_rle_pairs(const uint64_t *__restrict__ in, uint64_t n, const uint64_t *__restrict__ starts,
-                            const uint64_t *__restrict__ d_runs, uint64_t *__restrict__ out) {
-    const uint64_t runs = *d_runs;
-    for (uint64_t k = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < runs; k += uint64_t(gridDim.x) * blockDim.x) {
-        const uint64_t s = starts[k], e = k + 1 < runs ? starts[k + 1] : n;
-        out[2 * k] = in[s];
-        out[2 * k + 1] = e - s;
-    }
-}
-
-__global__ void k_rle_lengths(const uint64_t *__restrict__ pairs, uint64_t runs, uint64_t *__restrict__ lens) {
-    for (uint64_t k = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < runs; k += uint64_t(gridDim.x) * blockDim.x)
-        lens[k] = pairs[2 * k + 1];
-}
-
-// Expand runs: each CTA writes one tile of output rows; the tile's first
-// run is found by binary search over the run starts.
-__global__ void __launch_bounds__(256) k_rle_expand(const uint64_t *__restrict__ pairs,
-                                                   const uint64_t *__restrict__ rstart, uint64_t runs, uint64_t n,
-                                                   uint64_t *__restrict__ out) {
-    __shared__ uint64_t s_lo, s_hi;
-    const uint64_t t0 = uint64_t(blockIdx.x) * kRleTile;
-    if (t0 >= n) return;
-    const uint64_t t1 = minu(n, t0 + kRleTile);
-    if (threadIdx.x == 0) {
-        // last run with start <= t0
-        uint64_t lo = 0, hi = runs;
-        while (hi - lo > 1) {
-            uint64_t mid = (lo + hi) / 2;
-            if (rstart[mid] <= t0) lo = mid;
-            else hi = mid;
+    const unsigned excl_in_tile = wpre + incl - c;
+    uint64_t last_before_me = maxu(wlast, __shfl_up_sync(0xFFFFFFFFu, lmax, 1) * (lane > 0));
+    if (threadIdx.x == kRleThreads - 1) {
+        // the whole tile: runs and last head; publish, then look back
+        const uint64_t agg_runs = wpre + incl;
+        const uint64_t agg_last = maxu(last_before_me, my_last);
+        RleTileState *me = state + tile;
+        uint64_t excl_runs = 0, excl_last = kRleNone;
+        if (tile == 0) {
+            me->inc_runs = agg_runs;
+            me->inc_last = agg_last ? agg_last - 1 : kRleNone;
+            __threadfence();
+            atomicExch(&me->flag, kRleFlagInc);
+        } else {
+            me->agg_runs = agg_runs;
+            me->agg_last = agg_last ? agg_last - 1 : kRleNone;
+            __threadfence();
+            atomicExch(&me->flag, kRleFlagAgg);
+            bool ok = true;
+            for (uint64_t j = tile - 1;; j--) {
+                const RleTileState *o = state + j;
+                unsigned f = 0, spins = 0;
+                while ((f = *(volatile const unsigned *)&o->flag) == 0 && spins < kSpinLimit) spins++;
+                if (f == 0) {
+                    ok = false;
+                    break;
+                }
+                __threadfence();
+                const uint64_t cr = f == kRleFlagInc ? *(volatile const uint64_t *)&o->inc_runs
+                                                     : *(volatile const uint64_t *)&o->agg_runs;
+                const uint64_t cl = f == kRleFlagInc ? *(volatile const uint64_t *)&o->inc_last
+                                                     : *(volatile const uint64_t *)&o->agg_last;
+                excl_runs += cr;
+                if (excl_last == kRleNone) excl_last = cl;
+                if (f == kRleFlagInc || j == 0) break;
+            }
+            if (!ok) atomicOr(err, kErrTimeout);
+            me->inc_runs = excl_runs + agg_runs;
+            me->inc_last = agg_last ? agg_last - 1 : excl_last;
+            __threadfence();
+            atomicExch(&me->flag, kRleFlagInc);
         }
-        s_lo = lo;
-        lo = s_lo;
-        hi = runs;
-        while (hi - lo > 1) {
-            uint64_t mid = (lo + hi) / 2;
-            if (rstart[mid] <= t1 - 1) lo = mid;
-            else hi = mid;
+        s_excl_runs = excl_runs;
+        s_excl_last = excl_last;
+        if (tile == ntiles - 1) {
+            // the final run ends at row n
+            const uint64_t total = excl_runs + agg_runs;
+            const uint64_t last = agg_last ? agg_last - 1 : excl_last;
+            *d_runs = total;
+            if (total) out[2 * (total - 1) + 1] = n - last;
         }
-        s_hi = lo;
     }
     __syncthreads();
-    const uint64_t lo0 = s_lo, hi0 = s_hi;
-    for (uint64_t r = t0 + threadIdx.x; r < t1; r += blockDim.x) {
-        uint64_t lo = lo0, hi = hi0 + 1;
+    // pairs: value of every head's run, length of the run before it
+    uint64_t k = s_excl_runs + excl_in_tile;
+    uint64_t prev_head = last_before_me ? last_before_me - 1 : s_excl_last;
+#pragma unroll
+    for (unsigned j = 0; j < kRleRowsPerThread; j++) {
+        if ((m >> j) & 1u) {
+            const uint64_t r = r0 + j;
+            out[2 * k] = v[j];
+            if (k) out[2 * (k - 1) + 1] = r - prev_head;
+            prev_head = r;
+            k++;
+        }
+    }
+}
+
+// Decoder, pass 1: run lengths summed per tile of kRleTile runs.
+__global__ void __launch_bounds__(kRleThreads) k_rle_tile_rows(const uint64_t *__restrict__ pairs, uint64_t runs,
+                                                              uint64_t *__restrict__ tile_rows) {
+    __shared__ uint64_t s_w[kRleThreads / 32];
+    const uint64_t t = blockIdx.x, base = t * kRleTile;
+    uint64_t s = 0;
+    for (unsigned i = threadIdx.x; i < kRleTile; i += kRleThreads) {
+        const uint64_t r = base + i;
+        if (r < runs) s += __ldg(pairs + 2 * r + 1);
+    }
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) s += __shfl_xor_sync(0xFFFFFFFFu, s, d);
+    if ((threadIdx.x & 31u) == 0) s_w[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint64_t tot = 0;
+        for (unsigned w = 0; w < kRleThreads / 32; w++) tot += s_w[w];
+        tile_rows[t] = tot;
+    }
+}
+
+// Decoder, pass 2: each CTA writes kRleRows output rows.  It finds the run
+// tile holding its first row (binary search over the tiles' first rows),
+// loads that tile's values and run starts into shared memory (a scan of the
+// lengths), writes the rows the tile covers (each row's run by binary search
+// in shared memory) and moves on to the next tile until its rows are done.
+constexpr unsigned kRleRows = 8192;
+
+__global__ void __launch_bounds__(kRleThreads) k_rle_expand(const uint64_t *__restrict__ pairs, uint64_t runs,
+                                                           const uint64_t *__restrict__ tile_first, uint64_t ntiles,
+                                                           const uint64_t *__restrict__ total_rows, uint64_t n,
+                                                           uint64_t *__restrict__ out, unsigned *err) {
+    __shared__ uint64_t s_val[kRleTile];
+    __shared__ uint64_t s_start[kRleTile];
+    __shared__ uint64_t s_wsum[kRleThreads / 32];
+    __shared__ uint64_t s_t0;
+    const uint64_t row0 = uint64_t(blockIdx.x) * kRleRows;
+    if (row0 >= n) return;
+    const uint64_t row1 = minu(n, row0 + kRleRows);
+    const unsigned lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+    if (threadIdx.x == 0) {
+        uint64_t lo = 0, hi = ntiles;  // last tile whose first row <= row0
         while (hi - lo > 1) {
-            uint64_t mid = (lo + hi) / 2;
-            if (rstart[mid] <= r) lo = mid;
+            const uint64_t mid = (lo + hi) / 2;
+            if (tile_first[mid] <= row0) lo = mid;
             else hi = mid;
         }
-        out[r] = pairs[2 * lo];
+        s_t0 = lo;
     }
+    __syncthreads();
+    for (uint64_t t = s_t0; t < ntiles && tile_first[t] < row1; t++) {
+        const uint64_t rbase = t * kRleTile;
+        const unsigned nr = unsigned(minu(kRleTile, runs - rbase));
+        // this thread's kRleRowsPerThread runs: values and an exclusive scan of the lengths
+        const unsigned j0 = threadIdx.x * kRleRowsPerThread;
+        uint64_t len[kRleRowsPerThread], sum = 0;
+#pragma unroll
+        for (unsigned k = 0; k < kRleRowsPerThread; k++) {
+            const unsigned j = j0 + k;
+            len[k] = j < nr ? __ldg(pairs + 2 * (rbase + j) + 1) : 0;
+            s_val[j] = j < nr ? __ldg(pairs + 2 * (rbase + j)) : 0;
+            sum += len[k];
+        }
+        uint64_t incl = sum;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint64_t o = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+            if (int(lane) >= d) incl += o;
+        }
+        if (lane == 31) s_wsum[wid] = incl;
+        __syncthreads();
+        uint64_t run = tile_first[t] + incl - sum;
+        for (unsigned w = 0; w < wid; w++) run += s_wsum[w];
+#pragma unroll
+        for (unsigned k = 0; k < kRleRowsPerThread; k++) {
+            s_start[j0 + k] = j0 + k < nr ? run : ~uint64_t(0);
+            run += len[k];
+        }
+        __syncthreads();
+        const uint64_t tile_end = t + 1 < ntiles ? tile_first[t + 1] : n;
+        const uint64_t a = maxu(row0, tile_first[t]), b = minu(row1, tile_end);
+        for (uint64_t r = a + threadIdx.x; r < b; r += kRleThreads) {
+            unsigned lo = 0, hi = nr;  // last run of the tile with start <= r
+            while (hi - lo > 1) {
+                const unsigned mid = (lo + hi) >> 1;
+                if (s_start[mid] <= r) lo = mid;
+                else hi = mid;
+            }
+            out[r] = s_val[lo];
+        }
+        __syncthreads();
+    }
+    // the run lengths must add up to the column's length
+    if (blockIdx.x == 0 && threadIdx.x == 0 && *total_rows != n) atomicOr(err, kErrCorrupt);
 }
 
 }  // namespace
@@ -340,23 +472,20 @@ __global__ void __launch_bounds__(256) k_rle_expand(const uint64_t *__restrict__
 static int encode_rle(const uint64_t *d_in, uint64_t n, ms_col *out, ms_arena *a, cudaStream_t st) {
     const uint64_t tiles = (n + kRleTile - 1) / kRleTile;
     uint8_t *data = arena_take_t<uint8_t>(a, 16 * n + 64);
-    uint32_t *tc = arena_take_t<uint32_t>(a, tiles + 1);
-    uint64_t *toff = arena_take_t<uint64_t>(a, tiles + 1);
+    RleTileState *state = arena_take_t<RleTileState>(a, tiles + 1);
+    unsigned *ticket = arena_take_t<unsigned>(a, 2);
     uint64_t *d_runs = arena_take_t<uint64_t>(a, 1);
-    uint64_t *scr = arena_take_t<uint64_t>(a, scan_scratch_words(tiles, 1));
-    uint64_t *starts = arena_take_t<uint64_t>(a, n + 1);
-    if (!data || !tc || !toff || !d_runs || !scr || !starts) return ms_fail(MS_ERR_NOMEM, "arena exhausted (rle)");
+    if (!data || !state || !ticket || !d_runs) return ms_fail(MS_ERR_NOMEM, "arena exhausted (rle)");
     uint64_t runs = 0;
     if (n) {
-        k_rle_count<<<unsigned(tiles), 256, 0, st>>>(d_in, n, tc);
-        MS_CUDA_TRY(cudaGetLastError());
-        MS_CUDA_TRY((scan_exclusive<uint32_t, 1>(tc, tiles, toff, d_runs, scr, st)));
-        k_rle_starts<<<unsigned(tiles), 256, 0, st>>>(d_in, n, toff, starts);
-        MS_CUDA_TRY(cudaGetLastError());
-        k_rle_pairs<<<persistent_grid(256, 4), 256, 0, st>>>(d_in, n, starts, d_runs, (uint64_t *)data);
+        MS_CUDA_TRY(cudaMemsetAsync(state, 0, sizeof(RleTileState) * tiles, st));
+        MS_CUDA_TRY(cudaMemsetAsync(ticket, 0, sizeof(unsigned), st));
+        k_rle_encode<<<unsigned(tiles), kRleThreads, 0, st>>>(d_in, n, state, ticket, (uint64_t *)data, d_runs,
+                                                              a->d_err);
         MS_CUDA_TRY(cudaGetLastError());
         MS_CUDA_TRY(cudaMemcpyAsync(&runs, d_runs, 8, cudaMemcpyDeviceToHost, st));
-        MS_CUDA_TRY(cudaStreamSynchronize(st));
+        int rc = read_err(a, st);  // synchronises the stream
+        if (rc) return rc;
     }
     *out = ms_col{};
     out->format = MS_FMT_RLE;
@@ -372,16 +501,18 @@ static int decode_rle(const ms_col *in, uint64_t *d_out, ms_arena *a, cudaStream
     const uint64_t runs = in->size_used_byte / 16, n = in->count_values;
     if (!n) return MS_OK;
     if (!runs) return ms_fail(MS_ERR_CORRUPT, "rle column with values but no runs");
-    uint64_t *lens = arena_take_t<uint64_t>(a, runs + 1);
-    uint64_t *rstart = arena_take_t<uint64_t>(a, runs + 1);
+    const uint64_t tiles = (runs + kRleTile - 1) / kRleTile;
+    uint64_t *trows = arena_take_t<uint64_t>(a, tiles + 1);
+    uint64_t *tfirst = arena_take_t<uint64_t>(a, tiles + 1);
     uint64_t *tot = arena_take_t<uint64_t>(a, 1);
-    uint64_t *scr = arena_take_t<uint64_t>(a, scan_scratch_words(runs, 1));
-    if (!lens || !rstart || !tot || !scr) return ms_fail(MS_ERR_NOMEM, "arena exhausted (rle decode)");
-    k_rle_lengths<<<persistent_grid(256, 4), 256, 0, st>>>((const uint64_t *)in->data, runs, lens);
+    uint64_t *scr = arena_take_t<uint64_t>(a, scan_scratch_words(tiles, 1));
+    if (!trows || !tfirst || !tot || !scr) return ms_fail(MS_ERR_NOMEM, "arena exhausted (rle decode)");
+    const uint64_t *pairs = (const uint64_t *)in->data;
+    k_rle_tile_rows<<<unsigned(tiles), kRleThreads, 0, st>>>(pairs, runs, trows);
     MS_CUDA_TRY(cudaGetLastError());
-    MS_CUDA_TRY((scan_exclusive<uint64_t, 1>(lens, runs, rstart, tot, scr, st)));
-    const uint64_t tiles = (n + kRleTile - 1) / kRleTile;
-    k_rle_expand<<<unsigned(tiles), 256, 0, st>>>((const uint64_t *)in->data, rstart, runs, n, d_out);
+    MS_CUDA_TRY((scan_exclusive<uint64_t, 1>(trows, tiles, tfirst, tot, scr, st)));
+    const uint64_t chunks = (n + kRleRows - 1) / kRleRows;
+    k_rle_expand<<<unsigned(chunks), kRleThreads, 0, st>>>(pairs, runs, tfirst, tiles, tot, n, d_out, a->d_err);
     MS_CUDA_TRY(cudaGetLastError());
     return MS_OK;
 }

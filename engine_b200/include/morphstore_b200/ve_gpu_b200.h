@@ -341,7 +341,8 @@ template <class F> const column<uncompr_f> *agg_sum(const column<F> *in) {
                                                   auto *c = new column<uncompr_f>(sizeof(uint64_t));
                                                   check(ms_gpu_memcpy(c->get_data(), d_sum, 8, 1, 1, nullptr),
                                                         "agg_sum");
-                                                  c->set_meta_data(1, sizeof(uint64_t));
+                                                  // as agg_sum_compr.h:148-150 writes it
+                                                  c->set_meta_data(1, sizeof(uint64_t), sizeof(uint64_t));
                                                   return c;
                                               });
     dump("agg_sum", "out", out);

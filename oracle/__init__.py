@@ -297,6 +297,8 @@ class Reference:
         L.ref_intersect_scalar.argtypes = [U64P, C.c_uint64, U64P, C.c_uint64, U64P]
         L.ref_group.argtypes = [C.c_int, U8P, M, C.c_int, U8P, C.c_uint64, M, C.c_int, U8P, C.c_uint64, M]
         L.ref_agg_sum_grouped.argtypes = [U64P, U64P, C.c_uint64, C.c_uint64, U64P]
+        L.ref_bwi_compress.argtypes = [U64P, C.c_uint64, U8P, U8P, C.c_uint64, U64P]
+        L.ref_exhaustive_choose.argtypes = [U64P, C.c_uint64, U8P]
         L.ref_sps_prepare.restype = C.c_void_p
         L.ref_sps_prepare.argtypes = [U64P, U64P, C.c_uint64, U64P]
         L.ref_sps_run.restype = C.c_uint64
@@ -434,6 +436,33 @@ class Reference:
         out = np.zeros(max(n_groups, 1), dtype=np.uint64)
         self.lib.ref_agg_sum_grouped(gp, dp, len(d), n_groups, out.ctypes.data_as(U64P))
         return out[:n_groups]
+
+    def bwi_compress(self, values, codes):
+        """The reference's blockwise_individual_f<2048, …> container of
+        len(values)/2048 blocks, block b in the format with code codes[b]
+        (bytes as written; padding and for_f's unwritten header words are
+        zero here because the shim compresses into a zeroed buffer)."""
+        v, vp = _u64(values)
+        nblk = len(v) // 2048
+        c, cp = _u8(codes)
+        cap = 16 * len(v) + 128 * nblk + 4096
+        out = np.zeros(cap, dtype=np.uint8)
+        nb = C.c_uint64(0)
+        rc = self.lib.ref_bwi_compress(vp, nblk, cp, out.ctypes.data_as(U8P), cap, C.byref(nb))
+        if rc:
+            raise ValueError(f"ref_bwi_compress rc={rc}")
+        return out[: nb.value].copy()
+
+    def exhaustive_choose(self, values):
+        """The reference's exhaustive_size_format_selector's format code per
+        2048-value block (candidates: uncompr, static_vbp at the block's width,
+        dynamic_vbp, group_simple and the delta / for cascades over both)."""
+        v, vp = _u64(values)
+        nblk = len(v) // 2048
+        out = np.zeros(max(nblk, 1), dtype=np.uint8)
+        if self.lib.ref_exhaustive_choose(vp, nblk, out.ctypes.data_as(U8P)):
+            raise MemoryError("ref_exhaustive_choose")
+        return out[:nblk]
 
     def sps_prepare(self, x, y):
         """Compress x and y (dynamic_vbp) with the reference and keep them:

@@ -58,6 +58,52 @@ def mask_for_header(payload: np.ndarray, c: int) -> np.ndarray:
     return p
 
 
+def payload_size(data: np.ndarray, pay: int, c: int, code: int) -> int:
+    """Bytes of a block's payload at `pay` in candidate c, read from its
+    headers: static_vbp 256 bw; dynamic_vbp one 64-B page header with four
+    widths; delta+dvbp two such pages of two blocks; for+dvbp a 64-B header of
+    references and then two pages (rle: 16 B per run, runs not recorded)."""
+    if c == 0:
+        return 256 * code
+    if c == 1:
+        return 64 + 64 * int(data[pay:pay + 4].astype(np.int64).sum())
+    if c in (2, 3):
+        p = pay + (64 if c == 3 else 0)
+        for _ in range(2):
+            p += 64 + 64 * int(data[p:p + 2].astype(np.int64).sum())
+        return p - pay
+    raise ValueError("rle payloads carry no size header")
+
+
+def mask_container(data: np.ndarray, choice) -> np.ndarray:
+    """A blockwise_individual_f container's bytes with the padding after every
+    code byte and for_f's never-written header words zeroed: the reference
+    leaves both unwritten (blockwise_individual.h:189-196, for.h:214-220).
+    Blocks must not be rle (its payload has no size header)."""
+    x = np.array(data, dtype=np.uint8, copy=True)
+    pos = 0
+    for c in choice:
+        code_end = pos + 1
+        pay = (code_end + 63) // 64 * 64
+        x[code_end:pay] = 0
+        if int(c) == 3:
+            x[pay + 24:pay + 64] = 0
+        pos = pay + payload_size(x, pay, int(c), int(x[pos]))
+    if pos != len(x):
+        raise ValueError(f"container walk ends at {pos}, not at {len(x)}")
+    return x
+
+
+def shared_code(ref_code: int) -> int:
+    """The reference exhaustive selector's pick in the GPU's code space:
+    uncompr (chosen when a block needs all 64 bits) is static_vbp<64> there
+    (identical bytes); group_simple picks (66, 68, 70) have no GPU
+    counterpart and map to -1."""
+    if ref_code == 0:
+        return 64
+    return ref_code if ref_code <= 65 or ref_code in (67, 69) else -1
+
+
 def container_positions(sizes: np.ndarray):
     """(code byte offset, payload offset) per block and the total size."""
     q = np.zeros(len(sizes), dtype=np.int64)

@@ -21,6 +21,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
 import oracle as O  # noqa: E402
+from oracle import selector_ref as SR  # noqa: E402
 
 OUT = os.path.join(HERE, "golden.npz")
 
@@ -38,6 +39,35 @@ def inputs(orc):
     cols["uni64_9000"] = orc.uniform_bits(64, 64, 9000)
     cols["uni12_40077"] = orc.uniform_bits(12, 12, 40_077)
     return cols
+
+
+def bwi_inputs(orc):
+    """96 blocks of 2048 values (uniform over 1..64 bits, sorted with gaps,
+    runs, Zipf, constant), one pick per block cycling through static_vbp,
+    dynamic_vbp, delta+dvbp and for+dvbp (the formats the reference's
+    container and the GPU's share), and the format codes of those picks."""
+    from oracle import selector_ref as SR
+    geo, zipf = orc.geom_table(0.25), orc.zipf_table(1.2, 1 << 20)
+    blocks = []
+    for i in range(96):
+        kind = i % 6
+        if kind == 0:
+            blocks.append(orc.uniform_bits(700 + i, 1 + (i * 7) % 64, 2048))
+        elif kind == 1:
+            blocks.append(orc.sorted_gaps(700 + i, geo, 2048) + np.uint64(i << 30))
+        elif kind == 2:
+            blocks.append(orc.runs(700 + i, 5, 20, 2048))
+        elif kind == 3:
+            blocks.append(orc.from_table(700 + i, zipf, 2048))
+        elif kind == 4:
+            blocks.append(np.full(2048, i * 977, dtype=np.uint64))
+        else:
+            blocks.append(orc.uniform_bits(700 + i, 12, 2048) + np.uint64(1 << 40))
+    x = np.concatenate(blocks)
+    choice = np.array([(i * 5 + i // 4) % 4 for i in range(96)], dtype=np.uint8)
+    codes = np.array([SR.candidate_payload(orc, x[b * 2048:(b + 1) * 2048], int(choice[b]))[0] for b in range(96)],
+                     dtype=np.uint8)
+    return x, choice, codes
 
 
 def main():
@@ -151,6 +181,11 @@ def main():
     fx["group/ext_dvbp/bytes"] = O.mask_gap(O.DYNAMIC_VBP, 0, exb2, exm2, orc)
     fx["group/ext_dvbp/meta"] = np.array(exm2, dtype=np.uint64)
     fx["group/sum"] = ref.agg_sum_grouped(fx["group/gr"], meas, len(fx["group/ext"]))
+    # --- blockwise_individual_f and the exhaustive selector (ref_bwi.cpp) -------------------
+    x, choice, codes = bwi_inputs(orc)
+    fx["bwi/in"], fx["bwi/choice"], fx["bwi/codes"] = x, choice, codes
+    fx["bwi/bytes"] = SR.mask_container(ref.bwi_compress(x, codes), choice)
+    fx["bwi/exhaustive"] = ref.exhaustive_choose(x)
     np.savez_compressed(OUT, **fx)
     print(f"wrote {OUT}: {len(fx)} arrays, {os.path.getsize(OUT)} bytes")
 

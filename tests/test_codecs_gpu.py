@@ -138,3 +138,41 @@ def test_compact_keeps_column(ms, arena, orc, fmt):
     assert np.array_equal(k.to_numpy(), v)
     if fmt != O.RLE:
         assert ms.select_project_sum(k, ms.less, 1000, k) == ms.select_project_sum(c, ms.less, 1000, c)
+
+
+def _rle_cases(orc):
+    t = 2048  # the encoder's tile of rows
+    yield "every row a run", orc.uniform_bits(5, 40, 5 * t + 3)
+    yield "one run over many tiles", np.full(37 * t + 11, 123456789, dtype=np.uint64)
+    yield "two runs, boundary mid-tile", np.concatenate([np.full(9 * t + 700, 7, np.uint64),
+                                                           np.full(4 * t + 5, 9, np.uint64)])
+    yield "long geometric runs", orc.runs(6, 12, 20, 60 * t + 1)
+    yield "tile-sized lengths", orc.runs(7, 5, 20, 3 * t)
+    yield "one row", np.array([42], dtype=np.uint64)
+    yield "runs of 64-bit values", orc.runs(8, 3, 64, 10 * t + 9)
+    for k in (t - 1, t, t + 1, 2 * t - 1, 2 * t + 1):
+        yield f"runs, n={k}", orc.runs(9 + k, 2, 8, k)
+
+
+@pytest.mark.parametrize("case", range(12))
+def test_rle_codec_edge_cases(ms, arena, orc, case):
+    name, v = list(_rle_cases(orc))[case]
+    c = ms.morph(ms.Column.from_numpy(v, arena), ms.rle_f)
+    b, m = orc.compress(O.RLE, 0, v)
+    assert c.meta() == m, name
+    assert np.array_equal(c.raw_bytes(), b), name
+    assert np.array_equal(c.to_numpy(), v), name
+
+
+def test_rle_decode_reports_inconsistent_lengths(ms, arena, orc):
+    """Run lengths that do not add up to the column's count are a corrupt
+    column: the decoder writes only rows inside the runs (nothing out of
+    bounds) and the call reports MS_ERR_CORRUPT."""
+    v = orc.runs(3, 5, 20, 50_000)
+    b, m = orc.compress(O.RLE, 0, v)
+    pairs = b.view(np.uint64).copy()
+    pairs[1] -= 1  # the first run one row short
+    col = ms.Column.from_bytes(ms.rle_f, pairs.view(np.uint8), m, arena)
+    with pytest.raises(ms.MorphStoreError) as e:
+        ms.morph(col, ms.uncompr_f)
+    assert e.value.status == 5

@@ -123,7 +123,7 @@ def _device_values(ms, lib, arena, dist, seed, bits, tables):
 def test_codec_bytes_match_reference_at_2p28(ms, orc, reference_digests, case):
     import torch
     dist, fmt, bw, bits = case
-    arena = ms.Arena(14 << 30)
+    arena = ms.Arena(16 << 30)
     try:
         lib = ms.lib()
         tables = {}

@@ -145,3 +145,43 @@ def test_reference_known_answers(orc):
     assert list(gr) == eg and list(ext) == ee
     l, r, e = KATS["intersect"]
     assert list(orc.intersect_sorted(u(l), u(r))) == e
+
+
+def test_blockwise_container_restatement(orc):
+    """The restated blockwise_individual_f container (candidate payloads from
+    the C oracle, layout of blockwise_individual.h:169-311) equals the
+    reference's own container for the same per-block picks."""
+    from oracle import selector_ref as SR
+    x, choice, codes = FX["bwi/in"], FX["bwi/choice"], FX["bwi/codes"]
+    pays, got_codes = [], []
+    for b, c in enumerate(choice):
+        code, pay = SR.candidate_payload(orc, x[b * SR.BLOCK:(b + 1) * SR.BLOCK], int(c))
+        got_codes.append(code)
+        pays.append(pay)
+    assert np.array_equal(np.array(got_codes, dtype=np.uint8), codes)
+    sizes = np.array([len(p) for p in pays])
+    code_off, pay_off, total = SR.container_positions(sizes)
+    mine = np.zeros(total, dtype=np.uint8)
+    for b, pay in enumerate(pays):
+        mine[code_off[b]] = codes[b]
+        mine[pay_off[b]:pay_off[b] + len(pay)] = pay
+    assert np.array_equal(SR.mask_container(mine, choice), FX["bwi/bytes"])
+
+
+def test_exhaustive_choice_restatement(orc):
+    """Wherever the reference's exhaustive selector picks a format the GPU
+    also offers, the smallest of the restated candidates (static_vbp,
+    dynamic_vbp, delta+dvbp, for+dvbp; first one on ties, the reference's
+    order) is that format."""
+    from oracle import selector_ref as SR
+    x = FX["bwi/in"]
+    compared = 0
+    for b, rc in enumerate(FX["bwi/exhaustive"]):
+        want = SR.shared_code(int(rc))
+        if want < 0:
+            continue
+        cands = [SR.candidate_payload(orc, x[b * SR.BLOCK:(b + 1) * SR.BLOCK], c) for c in range(4)]
+        best = min(range(4), key=lambda c: (len(cands[c][1]), c))
+        assert cands[best][0] == want, (b, cands[best][0], want)
+        compared += 1
+    assert compared >= 40

@@ -148,3 +148,61 @@ def test_checkpoint_roundtrip(ms, arena, orc, sel, mixed):
     finally:
         a.close()
         b.close()
+
+
+# ---------------------------------------------------------------------------
+# blockwise_individual_f and the exhaustive selector against the reference
+# ---------------------------------------------------------------------------
+def _gpu_container(sel, arena, x, choice):
+    nblk = len(choice)
+    d = sel.to_device(arena, np.ascontiguousarray(x, dtype=np.uint64))
+    st, sz = sel.analyze(arena, d, nblk)
+    cont = sel.Container(arena, d, nblk, st, sel.to_device(arena, np.asarray(choice, dtype=np.uint8)))
+    codes = sel.to_host(cont.codes, nblk, np.uint8)
+    return R.mask_container(cont.host_bytes(), choice), codes, sel.to_host(sz, nblk * 5, np.uint32).reshape(nblk, 5), \
+        (d, st)
+
+
+def _restricted_codes(sel, arena, nblk, sizes, d_st):
+    """The GPU's exhaustive pick over the candidates the reference's container
+    shares (static_vbp, dynamic_vbp, delta+dvbp, for+dvbp; first on ties), as
+    format codes."""
+    best = np.argmin(sizes[:, :4], axis=1).astype(np.uint8)
+    d, st = d_st
+    cont = sel.Container(arena, d, nblk, st, sel.to_device(arena, best))
+    return sel.to_host(cont.codes, nblk, np.uint8)
+
+
+def test_blockwise_container_matches_reference_golden(ms, arena, sel):
+    from golden_util import load
+    fx = load()
+    if fx is None or "bwi/bytes" not in fx:
+        pytest.skip("golden fixtures missing")
+    got, codes, sizes, d_st = _gpu_container(sel, arena, fx["bwi/in"], fx["bwi/choice"])
+    assert np.array_equal(codes, fx["bwi/codes"])
+    assert np.array_equal(got, fx["bwi/bytes"])
+    want = np.array([R.shared_code(int(c)) for c in fx["bwi/exhaustive"]])
+    mine = _restricted_codes(sel, arena, len(want), sizes, d_st)
+    shared = want >= 0
+    assert shared.sum() >= 40
+    assert np.array_equal(mine[shared], want[shared])
+
+
+def test_blockwise_container_and_exhaustive_vs_reference_live(ms, arena, orc, ref, sel):
+    """4096 device-generated blocks of the four families: the GPU container
+    for random shared picks equals the reference's container byte for byte,
+    and the GPU's exhaustive choice agrees with the reference's selector
+    wherever the latter picks a shared format."""
+    if ref.isa != 512:
+        pytest.skip("the reference's AVX2 layouts differ from the device's")
+    nblk = 4096
+    d = sel.gen(arena, 29, nblk, 8, orc.zipf_table(1.2, 1 << 20))
+    x = sel.to_host(d, nblk * sel.BLOCK, np.uint64)
+    choice = np.random.default_rng(5).integers(0, 4, nblk).astype(np.uint8)
+    got, codes, sizes, d_st = _gpu_container(sel, arena, x, choice)
+    assert np.array_equal(got, R.mask_container(ref.bwi_compress(x, codes), choice))
+    want = np.array([R.shared_code(int(c)) for c in ref.exhaustive_choose(x)])
+    mine = _restricted_codes(sel, arena, nblk, sizes, d_st)
+    shared = want >= 0
+    assert shared.sum() >= nblk // 4
+    assert np.array_equal(mine[shared], want[shared])
