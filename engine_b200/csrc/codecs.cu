@@ -235,9 +235,9 @@ __global__ void __launch_bounds__(256) k_decode_all(ColView c, uint64_t *__restr
 // values).  Every head writes its run's value and the length of the run
 // before it; the last tile writes the length of the final run.  So the input
 // is read once and each pair written once (8 B/row + 16 B/run).
-constexpr unsigned kRleThreads = 256;
-constexpr unsigned kRleRowsPerThread = 8;
-constexpr unsigned kRleTile = kRleThreads * kRleRowsPerThread;
+constexpr unsigned kRleEncThreads = 1024;
+constexpr unsigned kRleRowsPerThread = 16;
+constexpr unsigned kRleEncTile = kRleEncThreads * kRleRowsPerThread;  // rows per encoder tile
 constexpr uint64_t kRleNone = ~uint64_t(0);
 enum : unsigned { kRleFlagAgg = 1, kRleFlagInc = 2 };
 
@@ -248,50 +248,82 @@ struct RleTileState {
     uint64_t inc_runs, inc_last;  // the same over tiles [0, this tile]
 };
 
-__global__ void __launch_bounds__(kRleThreads) k_rle_encode(const uint64_t *__restrict__ in, uint64_t n,
-                                                           RleTileState *state, unsigned *ticket,
-                                                           uint64_t *__restrict__ out, uint64_t *__restrict__ d_runs,
-                                                           unsigned *err) {
+// Warp-wide look-back (warp 0 of the tile): lane i inspects tile j - i, 32
+// predecessors per step; the nearest one with an inclusive prefix ends the
+// walk.  Returns false if a predecessor never published (bounded spin).
+__device__ bool rle_lookback(const RleTileState *state, uint64_t tile, uint64_t &excl_runs, uint64_t &excl_last) {
+    const unsigned lane = threadIdx.x & 31u;
+    excl_runs = 0;
+    excl_last = kRleNone;
+    for (int64_t j = int64_t(tile) - 1; j >= 0; j -= 32) {
+        const int64_t me = j - int64_t(lane);
+        unsigned f = kRleFlagInc;  // lanes before tile 0 act as an empty inclusive prefix
+        uint64_t cr = 0, cl = kRleNone;
+        if (me >= 0) {
+            const RleTileState *o = state + me;
+            unsigned spins = 0;
+            while ((f = *(volatile const unsigned *)&o->flag) == 0 && spins < kSpinLimit) spins++;
+            __threadfence();
+            cr = f == kRleFlagInc ? *(volatile const uint64_t *)&o->inc_runs : *(volatile const uint64_t *)&o->agg_runs;
+            cl = f == kRleFlagInc ? *(volatile const uint64_t *)&o->inc_last : *(volatile const uint64_t *)&o->agg_last;
+        }
+        if (__any_sync(0xFFFFFFFFu, f == 0)) return false;
+        const unsigned inc = __ballot_sync(0xFFFFFFFFu, f == kRleFlagInc);
+        const unsigned stop = inc ? unsigned(__ffs(inc) - 1) : 32u;  // lanes 0..stop count
+        const bool take = lane <= stop;
+        uint64_t r = take ? cr : 0;
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) r += __shfl_xor_sync(0xFFFFFFFFu, r, d);
+        excl_runs += r;
+        if (excl_last == kRleNone) {
+            // the nearest taken predecessor with a head
+            const unsigned has = __ballot_sync(0xFFFFFFFFu, take && cl != kRleNone);
+            if (has) excl_last = __shfl_sync(0xFFFFFFFFu, cl, __ffs(has) - 1);
+        }
+        if (inc) break;
+    }
+    return true;
+}
+
+__global__ void __launch_bounds__(kRleEncThreads) k_rle_encode(const uint64_t *__restrict__ in, uint64_t n,
+                                                              RleTileState *state, unsigned *ticket,
+                                                              uint64_t *__restrict__ out,
+                                                              uint64_t *__restrict__ d_runs, unsigned *err) {
+    constexpr unsigned NW = kRleEncThreads / 32, WR = 32 * kRleRowsPerThread;  // warps, rows per warp
     __shared__ uint64_t s_tile;
-    __shared__ unsigned s_wcnt[kRleThreads / 32];
-    __shared__ uint64_t s_wlast[kRleThreads / 32];
+    __shared__ unsigned s_wcnt[NW];
+    __shared__ uint64_t s_wlast[NW];
     __shared__ uint64_t s_excl_runs, s_excl_last;
     const unsigned lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
     if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
     __syncthreads();
     const uint64_t tile = s_tile;
-    const uint64_t ntiles = (n + kRleTile - 1) / kRleTile;
+    const uint64_t ntiles = (n + kRleEncTile - 1) / kRleEncTile;
     if (tile >= ntiles) return;
-    // this thread's rows and their heads
-    const uint64_t r0 = tile * kRleTile + uint64_t(threadIdx.x) * kRleRowsPerThread;
-    uint64_t v[kRleRowsPerThread];
-    uint64_t prev = r0 > 0 && r0 <= n ? __ldg(in + r0 - 1) : 0;
-    unsigned m = 0;
+    // warp w covers WR consecutive rows; in step k lane l reads row base + 32 k + l
+    // (one coalesced 256-byte load per step); heads as one ballot per step
+    const uint64_t base = tile * kRleEncTile + uint64_t(wid) * WR;
+    uint64_t carry = base > 0 && base <= n ? __ldg(in + base - 1) : 0;  // the row before the step's first
+    unsigned ball[kRleRowsPerThread];
+    unsigned c = 0;
 #pragma unroll
     for (unsigned k = 0; k < kRleRowsPerThread; k++) {
-        const uint64_t r = r0 + k;
-        v[k] = r < n ? __ldg(in + r) : 0;
-        if (r < n && (r == 0 || v[k] != prev)) m |= 1u << k;
-        prev = v[k];
+        const uint64_t r = base + 32 * k + lane;
+        const uint64_t v = r < n ? __ldg(in + r) : 0;
+        const uint64_t up = __shfl_up_sync(0xFFFFFFFFu, v, 1);
+        const uint64_t prev = lane ? up : carry;
+        carry = __shfl_sync(0xFFFFFFFFu, v, 31);
+        ball[k] = __ballot_sync(0xFFFFFFFFu, r < n && (r == 0 || v != prev));
+        c += __popc(ball[k]);
     }
-    const unsigned c = __popc(m);
-    // last head of this thread as row + 1 (0: none); rows grow with the thread
-    const uint64_t my_last = m ? r0 + (31 - __clz(m)) + 1 : 0;
-    // block-wide exclusive count scan and exclusive "last head before me"
-    unsigned incl = c;
-    uint64_t lmax = my_last;
+    // last head of this warp as row + 1 (0: none)
+    uint64_t my_last = 0;
 #pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        const unsigned t = __shfl_up_sync(0xFFFFFFFFu, incl, d);
-        const uint64_t tl = __shfl_up_sync(0xFFFFFFFFu, lmax, d);
-        if (int(lane) >= d) {
-            incl += t;
-            lmax = maxu(lmax, tl);
-        }
-    }
-    if (lane == 31) {
-        s_wcnt[wid] = incl;
-        s_wlast[wid] = lmax;
+    for (unsigned k = 0; k < kRleRowsPerThread; k++)
+        if (ball[k]) my_last = base + 32 * k + (31 - __clz(ball[k])) + 1;
+    if (lane == 0) {
+        s_wcnt[wid] = c;
+        s_wlast[wid] = my_last;
     }
     __syncthreads();
     unsigned wpre = 0;
@@ -300,73 +332,77 @@ __global__ void __launch_bounds__(kRleThreads) k_rle_encode(const uint64_t *__re
         wpre += s_wcnt[w];
         wlast = maxu(wlast, s_wlast[w]);
     }
-    const unsigned excl_in_tile = wpre + incl - c;
-    uint64_t last_before_me = maxu(wlast, __shfl_up_sync(0xFFFFFFFFu, lmax, 1) * (lane > 0));
-    if (threadIdx.x == kRleThreads - 1) {
+    if (wid == 0) {
         // the whole tile: runs and last head; publish, then look back
-        const uint64_t agg_runs = wpre + incl;
-        const uint64_t agg_last = maxu(last_before_me, my_last);
+        uint64_t agg_runs = 0, agg_last = 0;
+        for (unsigned w = 0; w < NW; w++) {
+            agg_runs += s_wcnt[w];
+            agg_last = maxu(agg_last, s_wlast[w]);
+        }
         RleTileState *me = state + tile;
+        const uint64_t own_last = agg_last ? agg_last - 1 : kRleNone;
         uint64_t excl_runs = 0, excl_last = kRleNone;
         if (tile == 0) {
-            me->inc_runs = agg_runs;
-            me->inc_last = agg_last ? agg_last - 1 : kRleNone;
-            __threadfence();
-            atomicExch(&me->flag, kRleFlagInc);
-        } else {
-            me->agg_runs = agg_runs;
-            me->agg_last = agg_last ? agg_last - 1 : kRleNone;
-            __threadfence();
-            atomicExch(&me->flag, kRleFlagAgg);
-            bool ok = true;
-            for (uint64_t j = tile - 1;; j--) {
-                const RleTileState *o = state + j;
-                unsigned f = 0, spins = 0;
-                while ((f = *(volatile const unsigned *)&o->flag) == 0 && spins < kSpinLimit) spins++;
-                if (f == 0) {
-                    ok = false;
-                    break;
-                }
+            if (lane == 0) {
+                me->inc_runs = agg_runs;
+                me->inc_last = own_last;
                 __threadfence();
-                const uint64_t cr = f == kRleFlagInc ? *(volatile const uint64_t *)&o->inc_runs
-                                                     : *(volatile const uint64_t *)&o->agg_runs;
-                const uint64_t cl = f == kRleFlagInc ? *(volatile const uint64_t *)&o->inc_last
-                                                     : *(volatile const uint64_t *)&o->agg_last;
-                excl_runs += cr;
-                if (excl_last == kRleNone) excl_last = cl;
-                if (f == kRleFlagInc || j == 0) break;
+                atomicExch(&me->flag, kRleFlagInc);
             }
-            if (!ok) atomicOr(err, kErrTimeout);
-            me->inc_runs = excl_runs + agg_runs;
-            me->inc_last = agg_last ? agg_last - 1 : excl_last;
-            __threadfence();
-            atomicExch(&me->flag, kRleFlagInc);
+        } else {
+            if (lane == 0) {
+                me->agg_runs = agg_runs;
+                me->agg_last = own_last;
+                __threadfence();
+                atomicExch(&me->flag, kRleFlagAgg);
+            }
+            __syncwarp();
+            if (!rle_lookback(state, tile, excl_runs, excl_last) && lane == 0) atomicOr(err, kErrTimeout);
+            if (lane == 0) {
+                me->inc_runs = excl_runs + agg_runs;
+                me->inc_last = own_last != kRleNone ? own_last : excl_last;
+                __threadfence();
+                atomicExch(&me->flag, kRleFlagInc);
+            }
         }
-        s_excl_runs = excl_runs;
-        s_excl_last = excl_last;
-        if (tile == ntiles - 1) {
-            // the final run ends at row n
-            const uint64_t total = excl_runs + agg_runs;
-            const uint64_t last = agg_last ? agg_last - 1 : excl_last;
-            *d_runs = total;
-            if (total) out[2 * (total - 1) + 1] = n - last;
+        if (lane == 0) {
+            s_excl_runs = excl_runs;
+            s_excl_last = excl_last;
+            if (tile == ntiles - 1) {
+                // the final run ends at row n
+                const uint64_t total = excl_runs + agg_runs;
+                const uint64_t last = own_last != kRleNone ? own_last : excl_last;
+                *d_runs = total;
+                if (total) out[2 * (total - 1) + 1] = n - last;
+            }
         }
     }
     __syncthreads();
-    // pairs: value of every head's run, length of the run before it
-    uint64_t k = s_excl_runs + excl_in_tile;
-    uint64_t prev_head = last_before_me ? last_before_me - 1 : s_excl_last;
+    // pairs: every head writes its run's value and the length of the run
+    // before it; consecutive lanes write consecutive pairs
+    uint64_t k_run = s_excl_runs + wpre;                       // run index of the warp's next head
+    uint64_t prev_head = wlast ? wlast - 1 : s_excl_last;      // row of the head before it
+    const unsigned below = (1u << lane) - 1u;
 #pragma unroll
-    for (unsigned j = 0; j < kRleRowsPerThread; j++) {
-        if ((m >> j) & 1u) {
-            const uint64_t r = r0 + j;
-            out[2 * k] = v[j];
-            if (k) out[2 * (k - 1) + 1] = r - prev_head;
-            prev_head = r;
-            k++;
+    for (unsigned k = 0; k < kRleRowsPerThread; k++) {
+        const unsigned bk = ball[k];
+        if (!bk) continue;
+        const uint64_t r = base + 32 * k + lane;
+        if ((bk >> lane) & 1u) {
+            const uint64_t idx = k_run + __popc(bk & below);
+            const unsigned lower = bk & below;
+            const uint64_t ph = lower ? base + 32 * k + (31 - __clz(lower)) : prev_head;
+            out[2 * idx] = __ldg(in + r);
+            if (idx) out[2 * (idx - 1) + 1] = r - ph;
         }
+        k_run += __popc(bk);
+        prev_head = base + 32 * k + (31 - __clz(bk));
     }
 }
+
+constexpr unsigned kRleThreads = 256;
+constexpr unsigned kRleRunsPerThread = 8;
+constexpr unsigned kRleTile = kRleThreads * kRleRunsPerThread;  // runs per decoder tile
 
 // Decoder, pass 1: run lengths summed per tile of kRleTile runs.
 __global__ void __launch_bounds__(kRleThreads) k_rle_tile_rows(const uint64_t *__restrict__ pairs, uint64_t runs,
@@ -389,46 +425,59 @@ __global__ void __launch_bounds__(kRleThreads) k_rle_tile_rows(const uint64_t *_
     }
 }
 
-// Decoder, pass 2: each CTA writes kRleRows output rows.  It finds the run
-// tile holding its first row (binary search over the tiles' first rows),
-// loads that tile's values and run starts into shared memory (a scan of the
-// lengths), writes the rows the tile covers (each row's run by binary search
-// in shared memory) and moves on to the next tile until its rows are done.
+// Decoder, pass 2: the run tile holding the first row of every chunk of
+// kRleRows output rows (one thread per chunk, binary search over the tiles'
+// first rows).
 constexpr unsigned kRleRows = 8192;
 
-__global__ void __launch_bounds__(kRleThreads) k_rle_expand(const uint64_t *__restrict__ pairs, uint64_t runs,
-                                                           const uint64_t *__restrict__ tile_first, uint64_t ntiles,
-                                                           const uint64_t *__restrict__ total_rows, uint64_t n,
-                                                           uint64_t *__restrict__ out, unsigned *err) {
-    __shared__ uint64_t s_val[kRleTile];
-    __shared__ uint64_t s_start[kRleTile];
-    __shared__ uint64_t s_wsum[kRleThreads / 32];
-    __shared__ uint64_t s_t0;
-    const uint64_t row0 = uint64_t(blockIdx.x) * kRleRows;
-    if (row0 >= n) return;
-    const uint64_t row1 = minu(n, row0 + kRleRows);
-    const unsigned lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
-    if (threadIdx.x == 0) {
+__global__ void k_rle_chunk_tiles(const uint64_t *__restrict__ tile_first, uint64_t ntiles, uint64_t chunks,
+                                  uint32_t *__restrict__ chunk_tile) {
+    for (uint64_t c = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; c < chunks; c += uint64_t(gridDim.x) * blockDim.x) {
+        const uint64_t row0 = c * kRleRows;
         uint64_t lo = 0, hi = ntiles;  // last tile whose first row <= row0
         while (hi - lo > 1) {
             const uint64_t mid = (lo + hi) / 2;
             if (tile_first[mid] <= row0) lo = mid;
             else hi = mid;
         }
-        s_t0 = lo;
+        chunk_tile[c] = uint32_t(lo);
     }
-    __syncthreads();
-    for (uint64_t t = s_t0; t < ntiles && tile_first[t] < row1; t++) {
+}
+
+// Decoder, pass 3: each CTA writes kRleRows output rows.  Starting at the
+// run tile that holds its first row,
+// loads that tile's values and run starts into shared memory (a scan of the
+// lengths), writes the rows the tile covers (each row's run by binary search
+// in shared memory) and moves on to the next tile until its rows are done.
+__global__ void __launch_bounds__(kRleThreads) k_rle_expand(const uint64_t *__restrict__ pairs, uint64_t runs,
+                                                           const uint64_t *__restrict__ tile_first, uint64_t ntiles,
+                                                           const uint32_t *__restrict__ chunk_tile,
+                                                           const uint64_t *__restrict__ total_rows, uint64_t n,
+                                                           uint64_t *__restrict__ out, unsigned *err) {
+    __shared__ uint64_t s_val[kRleTile];
+    __shared__ uint64_t s_start[kRleTile];
+    __shared__ uint64_t s_wsum[kRleThreads / 32];
+    const uint64_t row0 = uint64_t(blockIdx.x) * kRleRows;
+    if (row0 >= n) return;
+    const uint64_t row1 = minu(n, row0 + kRleRows);
+    const unsigned lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+    for (uint64_t t = chunk_tile[blockIdx.x]; t < ntiles && tile_first[t] < row1; t++) {
         const uint64_t rbase = t * kRleTile;
         const unsigned nr = unsigned(minu(kRleTile, runs - rbase));
-        // this thread's kRleRowsPerThread runs: values and an exclusive scan of the lengths
-        const unsigned j0 = threadIdx.x * kRleRowsPerThread;
-        uint64_t len[kRleRowsPerThread], sum = 0;
+        // the tile's pairs into shared memory, one 16-byte pair per thread and step
+        for (unsigned j = threadIdx.x; j < kRleTile; j += kRleThreads) {
+            const ulonglong2 pr = j < nr ? __ldg(reinterpret_cast<const ulonglong2 *>(pairs) + rbase + j)
+                                         : make_ulonglong2(0, 0);
+            s_val[j] = pr.x;
+            s_start[j] = pr.y;
+        }
+        __syncthreads();
+        // this thread's kRleRunsPerThread consecutive runs: an exclusive scan of the lengths
+        const unsigned j0 = threadIdx.x * kRleRunsPerThread;
+        uint64_t len[kRleRunsPerThread], sum = 0;
 #pragma unroll
-        for (unsigned k = 0; k < kRleRowsPerThread; k++) {
-            const unsigned j = j0 + k;
-            len[k] = j < nr ? __ldg(pairs + 2 * (rbase + j) + 1) : 0;
-            s_val[j] = j < nr ? __ldg(pairs + 2 * (rbase + j)) : 0;
+        for (unsigned k = 0; k < kRleRunsPerThread; k++) {
+            len[k] = s_start[j0 + k];
             sum += len[k];
         }
         uint64_t incl = sum;
@@ -442,7 +491,7 @@ __global__ void __launch_bounds__(kRleThreads) k_rle_expand(const uint64_t *__re
         uint64_t run = tile_first[t] + incl - sum;
         for (unsigned w = 0; w < wid; w++) run += s_wsum[w];
 #pragma unroll
-        for (unsigned k = 0; k < kRleRowsPerThread; k++) {
+        for (unsigned k = 0; k < kRleRunsPerThread; k++) {
             s_start[j0 + k] = j0 + k < nr ? run : ~uint64_t(0);
             run += len[k];
         }
@@ -470,7 +519,7 @@ __global__ void __launch_bounds__(kRleThreads) k_rle_expand(const uint64_t *__re
 // host drivers
 // ---------------------------------------------------------------------------
 static int encode_rle(const uint64_t *d_in, uint64_t n, ms_col *out, ms_arena *a, cudaStream_t st) {
-    const uint64_t tiles = (n + kRleTile - 1) / kRleTile;
+    const uint64_t tiles = (n + kRleEncTile - 1) / kRleEncTile;
     uint8_t *data = arena_take_t<uint8_t>(a, 16 * n + 64);
     RleTileState *state = arena_take_t<RleTileState>(a, tiles + 1);
     unsigned *ticket = arena_take_t<unsigned>(a, 2);
@@ -480,8 +529,8 @@ static int encode_rle(const uint64_t *d_in, uint64_t n, ms_col *out, ms_arena *a
     if (n) {
         MS_CUDA_TRY(cudaMemsetAsync(state, 0, sizeof(RleTileState) * tiles, st));
         MS_CUDA_TRY(cudaMemsetAsync(ticket, 0, sizeof(unsigned), st));
-        k_rle_encode<<<unsigned(tiles), kRleThreads, 0, st>>>(d_in, n, state, ticket, (uint64_t *)data, d_runs,
-                                                              a->d_err);
+        k_rle_encode<<<unsigned(tiles), kRleEncThreads, 0, st>>>(d_in, n, state, ticket, (uint64_t *)data, d_runs,
+                                                                 a->d_err);
         MS_CUDA_TRY(cudaGetLastError());
         MS_CUDA_TRY(cudaMemcpyAsync(&runs, d_runs, 8, cudaMemcpyDeviceToHost, st));
         int rc = read_err(a, st);  // synchronises the stream
@@ -512,7 +561,12 @@ static int decode_rle(const ms_col *in, uint64_t *d_out, ms_arena *a, cudaStream
     MS_CUDA_TRY(cudaGetLastError());
     MS_CUDA_TRY((scan_exclusive<uint64_t, 1>(trows, tiles, tfirst, tot, scr, st)));
     const uint64_t chunks = (n + kRleRows - 1) / kRleRows;
-    k_rle_expand<<<unsigned(chunks), kRleThreads, 0, st>>>(pairs, runs, tfirst, tiles, tot, n, d_out, a->d_err);
+    uint32_t *ctile = arena_take_t<uint32_t>(a, chunks + 1);
+    if (!ctile) return ms_fail(MS_ERR_NOMEM, "arena exhausted (rle decode)");
+    k_rle_chunk_tiles<<<unsigned(minu((chunks + 255) / 256, uint64_t(persistent_grid(256, 4)))), 256, 0, st>>>(
+        tfirst, tiles, chunks, ctile);
+    MS_CUDA_TRY(cudaGetLastError());
+    k_rle_expand<<<unsigned(chunks), kRleThreads, 0, st>>>(pairs, runs, tfirst, tiles, ctile, tot, n, d_out, a->d_err);
     MS_CUDA_TRY(cudaGetLastError());
     return MS_OK;
 }

@@ -348,6 +348,130 @@ __device__ __forceinline__ uint64_t sum32_block_rt(unsigned bw, const uint64_t *
 
 namespace ms {
 
+// ---------------------------------------------------------------------------
+// Selection flags: the predicate of x and the sum over y meet in 32 flags
+// (0 or 1, one register per value of the half) instead of a bit mask, so
+// the y side multiplies-and-adds (s += v * flag, an integer multiply-add)
+// rather than testing a mask bit and adding under a predicate, and fields are
+// isolated as (w << a) >> b.  Both moves take work off the integer ALU,
+// which bounds the fused kernel.
+// ---------------------------------------------------------------------------
+template <unsigned BW, bool kFlip>
+__device__ __forceinline__ unsigned vbp_sel32_top(const uint64_t *__restrict__ blk, unsigned l, unsigned h,
+                                                  uint32_t T, uint32_t (&sel)[32]) {
+    static_assert(BW <= 32, "32-bit fields");
+    constexpr unsigned NW = (32 * BW + 63) / 64 + 1;
+    constexpr unsigned NH = BW + 1;
+    const unsigned sbit = 32u * h * BW;
+    const unsigned w0 = sbit >> 6;
+    uint32_t hw[2 * NW];
+#pragma unroll
+    for (unsigned i = 0; i < NW; i++) {
+        const uint64_t w = (w0 + i < BW) ? blk[(w0 + i) * 8 + l] : 0;
+        hw[2 * i] = uint32_t(w);
+        hw[2 * i + 1] = uint32_t(w >> 32);
+    }
+    const unsigned o = (sbit >> 5) & 1u;
+    uint32_t n[NH];
+#pragma unroll
+    for (unsigned i = 0; i < NH; i++) {
+        if (BW % 2 == 0) n[i] = (i < 2 * NW) ? hw[i] : 0;
+        else n[i] = (i + 1 < 2 * NW) ? (o ? hw[i + 1] : hw[i]) : ((i < 2 * NW && !o) ? hw[i] : 0);
+    }
+    const uint32_t Tt = BW == 32 ? T : (T << (32u - BW));
+    unsigned c0 = 0, c1 = 0;
+#pragma unroll
+    for (unsigned k = 0; k < 32; k++) {
+        const unsigned p = k * BW, wi = p >> 5, sh = p & 31u;
+        const uint32_t top = (sh + BW <= 32) ? (n[wi] << (32u - sh - BW)) : __funnelshift_r(n[wi], n[wi + 1], sh + BW - 32u);
+        const bool lt = top < Tt;
+        sel[k] = (kFlip ? !lt : lt) ? 1u : 0u;
+        if (k & 1) c1 += sel[k];
+        else c0 += sel[k];
+    }
+    return c0 + c1;
+}
+
+// Flags of the 32 values of half h of lane l of a plain vbp block of width
+// bw; returns how many are set.  bw 0 or > 64 sets *bad.
+__device__ __forceinline__ unsigned sel32_block_rt(unsigned bw, const uint64_t *blk, unsigned l, unsigned h,
+                                                   const Pred &p, uint32_t (&sel)[32], bool &bad) {
+    if (bw >= 1 && bw <= 32 && !p.is_eq && p.T < (uint64_t(1) << bw)) {
+        switch (bw) {
+#define MS_X(B)                                                                                              \
+    case B:                                                                                                  \
+        return p.flip ? vbp_sel32_top<(B <= 32 ? B : 32), true>(blk, l, h, uint32_t(p.T), sel)               \
+                      : vbp_sel32_top<(B <= 32 ? B : 32), false>(blk, l, h, uint32_t(p.T), sel);
+            MS_X(1) MS_X(2) MS_X(3) MS_X(4) MS_X(5) MS_X(6) MS_X(7) MS_X(8) MS_X(9) MS_X(10) MS_X(11) MS_X(12)
+            MS_X(13) MS_X(14) MS_X(15) MS_X(16) MS_X(17) MS_X(18) MS_X(19) MS_X(20) MS_X(21) MS_X(22) MS_X(23)
+            MS_X(24) MS_X(25) MS_X(26) MS_X(27) MS_X(28) MS_X(29) MS_X(30) MS_X(31) MS_X(32)
+#undef MS_X
+        default: break;
+        }
+    }
+    const unsigned m = mask32_block_rt(bw, blk, l, h, p, bad);
+#pragma unroll
+    for (unsigned k = 0; k < 32; k++) sel[k] = (m >> k) & 1u;
+    return __popc(m);
+}
+
+// Sum of the flagged values among the 32 of half h of lane l (BW <= 26, so
+// the 32-bit partial cannot overflow).
+template <unsigned BW>
+__device__ __forceinline__ uint32_t sum32_sel(const uint64_t *__restrict__ blk, unsigned l, unsigned h,
+                                              const uint32_t (&sel)[32]) {
+    static_assert(BW <= 26, "32-bit partial sums");
+    constexpr unsigned NW = (32 * BW + 63) / 64 + 1;
+    constexpr unsigned NH = BW + 1;
+    const unsigned sbit = 32u * h * BW;
+    const unsigned w0 = sbit >> 6;
+    uint32_t hw[2 * NW];
+#pragma unroll
+    for (unsigned i = 0; i < NW; i++) {
+        const uint64_t w = (w0 + i < BW) ? blk[(w0 + i) * 8 + l] : 0;
+        hw[2 * i] = uint32_t(w);
+        hw[2 * i + 1] = uint32_t(w >> 32);
+    }
+    const unsigned o = (sbit >> 5) & 1u;
+    uint32_t n[NH];
+#pragma unroll
+    for (unsigned i = 0; i < NH; i++) {
+        if (BW % 2 == 0) n[i] = (i < 2 * NW) ? hw[i] : 0;
+        else n[i] = (i + 1 < 2 * NW) ? (o ? hw[i + 1] : hw[i]) : ((i < 2 * NW && !o) ? hw[i] : 0);
+    }
+    uint32_t s0 = 0, s1 = 0;
+#pragma unroll
+    for (unsigned k = 0; k < 32; k++) {
+        const unsigned p = k * BW, wi = p >> 5, sh = p & 31u;
+        const uint32_t top = (sh + BW <= 32) ? (n[wi] << (32u - sh - BW)) : __funnelshift_r(n[wi], n[wi + 1], sh + BW - 32u);
+        const uint32_t v = top >> (32u - BW);
+        if (k & 1) s1 += v * sel[k];
+        else s0 += v * sel[k];
+    }
+    return s0 + s1;
+}
+
+__device__ __forceinline__ uint64_t sum32_sel_rt(unsigned bw, const uint64_t *blk, unsigned l, unsigned h,
+                                                 const uint32_t (&sel)[32], bool &bad) {
+    switch (bw) {
+#define MS_X(B) \
+    case B: return sum32_sel<(B <= 26 ? B : 26)>(blk, l, h, sel);
+        MS_X(1) MS_X(2) MS_X(3) MS_X(4) MS_X(5) MS_X(6) MS_X(7) MS_X(8) MS_X(9) MS_X(10) MS_X(11) MS_X(12) MS_X(13)
+        MS_X(14) MS_X(15) MS_X(16) MS_X(17) MS_X(18) MS_X(19) MS_X(20) MS_X(21) MS_X(22) MS_X(23) MS_X(24) MS_X(25)
+        MS_X(26)
+#undef MS_X
+    default: break;
+    }
+    unsigned m = 0;
+#pragma unroll
+    for (unsigned k = 0; k < 32; k++) m |= sel[k] << k;
+    return sum32_block_rt(bw, blk, l, h, m, bad);
+}
+
+}  // namespace ms
+
+namespace ms {
+
 // Select and sum over the same plain vbp block, decoded once: cnt gets the
 // number of rows of thread (l, q) that pass, the return value their sum.
 template <unsigned BW>

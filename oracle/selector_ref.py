@@ -3,8 +3,9 @@
 * candidate payloads of a 2048-value block (the bytes the reference's
   morph_batch writes for each candidate, via the C oracle);
 * the sampled statistics the learned selector reads (engine's k_sel_features);
-* the MLP's forward pass and gradients in float64 with BF16-rounded weights,
-  to check the GPU training kernels;
+* the MLP's forward pass and gradients in float64 with the GPU's BF16
+  rounding points (weights, and every matrix-product input), to check the
+  tensor-core training kernels;
 * the blockwise container layout (blockwise_individual.h:169-311).
 """
 from __future__ import annotations
@@ -182,25 +183,37 @@ def unpack(params: np.ndarray):
     return out
 
 
-def loss_and_grads(params: np.ndarray, feats: np.ndarray, sizes: np.ndarray):
-    """Loss and gradient (parameter order) for a batch, float64 arithmetic on
-    BF16-rounded weights."""
+def forward(params: np.ndarray, feats: np.ndarray) -> np.ndarray:
+    """Predicted log2 sizes, with the GPU's rounding points (see below)."""
     w = unpack(bf16(params))
-    x = feats.astype(np.float64)
+    r = lambda a: bf16(a.astype(np.float32)).astype(np.float64)  # noqa: E731
+    h1 = r(np.maximum(r(feats) @ w["W1"].T + w["b1"], 0))
+    h2 = r(np.maximum(h1 @ w["W2"].T + w["b2"], 0))
+    return h2 @ w["W3"].T + w["b3"]
+
+
+def loss_and_grads(params: np.ndarray, feats: np.ndarray, sizes: np.ndarray):
+    """Loss and gradient (parameter order) for a batch, float64 arithmetic
+    with the GPU's rounding points: BF16 weights; features, hidden
+    activations and backward deltas rounded to BF16 where they enter a matrix
+    product; biases, ReLU masks and bias gradients on the unrounded values."""
+    w = unpack(bf16(params))
+    r = lambda a: bf16(a.astype(np.float32)).astype(np.float64)  # noqa: E731
+    x = r(feats)
     y = np.log2(sizes.astype(np.float64))
     z1 = x @ w["W1"].T + w["b1"]
-    h1 = np.maximum(z1, 0)
+    h1 = r(np.maximum(z1, 0))
     z2 = h1 @ w["W2"].T + w["b2"]
-    h2 = np.maximum(z2, 0)
+    h2 = r(np.maximum(z2, 0))
     o = h2 @ w["W3"].T + w["b3"]
     e = o - y
     B = len(x)
     loss = (e ** 2).sum() / (B * OUT)
     do = 2 * e / (B * OUT)
-    g = {"W3": do.T @ h2, "b3": do.sum(0)}
-    d2 = (do @ w["W3"]) * (z2 > 0)
-    g["W2"], g["b2"] = d2.T @ h1, d2.sum(0)
-    d1 = (d2 @ w["W2"]) * (z1 > 0)
-    g["W1"], g["b1"] = d1.T @ x, d1.sum(0)
+    g = {"W3": r(do).T @ h2, "b3": do.sum(0)}
+    d2 = (r(do) @ w["W3"]) * (z2 > 0)
+    g["W2"], g["b2"] = r(d2).T @ h1, d2.sum(0)
+    d1 = (r(d2) @ w["W2"]) * (z1 > 0)
+    g["W1"], g["b1"] = r(d1).T @ x, d1.sum(0)
     flat = np.concatenate([g[name].ravel() for name, _ in LAYOUT])
     return loss, flat

@@ -100,6 +100,33 @@ def test_mlp_gradients_match_cpu(ms, arena, sel, mixed):
         m.close()
 
 
+def test_mlp_predictions_match_cpu(ms, arena, sel, mixed):
+    """The tensor-core forward pass (k_mlp_choose) against the float64
+    restatement with the same BF16 rounding points, after a few training
+    steps so that every layer carries signal; also the choice and the
+    fallback decision derived from the predictions."""
+    d, nblk, x = mixed
+    _, sz = sel.analyze(arena, d, nblk)
+    fd = sel.features(arena, d, nblk)
+    m = sel.Mlp(seed=9, max_batch=256)
+    try:
+        m.train(arena, fd, sz, nblk, steps=30, batch=96)
+        margin = 0.05
+        ch, nf, pr = m.choose(arena, fd, nblk, margin, want_pred=True)
+        got = sel.to_host(pr, nblk * 5, np.float32).reshape(nblk, 5)
+        feats = sel.to_host(fd, nblk * 32, np.float32).reshape(nblk, 32)
+        want = R.forward(m.params(), feats)
+        np.testing.assert_allclose(got, want, rtol=1e-3, atol=2e-2)
+        choice = sel.to_host(ch, nblk, np.uint8)
+        srt = np.sort(got, axis=1)
+        unsure = srt[:, 1] - srt[:, 0] < margin
+        assert np.array_equal(choice == 255, unsure)
+        assert np.array_equal(choice[~unsure], np.argmin(got, axis=1)[~unsure])
+        assert int(sel.to_host(nf, 1, np.uint64)[0]) == int(unsure.sum())
+    finally:
+        m.close()
+
+
 def _dataset(ms, arena, orc, sel, seed, nblk):
     d = sel.gen(arena, seed, nblk, 32, orc.zipf_table(1.2, 1 << 20))
     st, sz = sel.analyze(arena, d, nblk)
