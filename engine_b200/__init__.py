@@ -94,6 +94,8 @@ _sig = {
     "ms_gpu_batch_create": (C.c_int, [_P(MsCol), _V, _U64, C.c_int, _V, _P(_V), _V]),
     "ms_gpu_batch_set_config": (C.c_int, [_V, _P(MsTuning)]),
     "ms_gpu_batch_get_config": (C.c_int, [_V, _P(MsTuning)]),
+    "ms_gpu_batch_set_kind_config": (C.c_int, [_V, C.c_int, _P(MsTuning)]),
+    "ms_gpu_batch_get_kind_config": (C.c_int, [_V, C.c_int, _P(MsTuning), _P(_U64)]),
     "ms_gpu_batch_run": (C.c_int, [_V, _V, _V, _V]),
     "ms_gpu_batch_run_graph": (C.c_int, [_V, _V, _V, _V]),
     "ms_gpu_batch_info": (C.c_int, [_V, _P(_U64), _P(_U64)]),
@@ -102,6 +104,8 @@ _sig = {
     "ms_gpu_get_tuning": (C.c_int, [_P(MsTuning)]),
     "ms_gpu_gen_uniform_bits": (C.c_int, [_U64, C.c_uint, _U64, _V, _V]),
     "ms_gpu_gen_uniform_bits_at": (C.c_int, [_U64, C.c_uint, _U64, _U64, _V, _V]),
+    "ms_gpu_col_slice": (C.c_int, [_P(MsCol), _U64, _U64, _V, _P(MsCol)]),
+    "ms_gpu_delta_lane_sums": (C.c_int, [_P(MsCol), _V, _V, _V]),
     "ms_gpu_gen_from_table": (C.c_int, [_U64, _V, _U64, _U64, _V, _V]),
     "ms_gpu_gen_sorted_gaps": (C.c_int, [_U64, _V, _U64, _U64, _V, _V, _V]),
     "ms_gpu_gen_runs": (C.c_int, [_U64, C.c_uint, C.c_uint, _U64, _V, _V, _V]),
@@ -353,6 +357,25 @@ class Column:
                "col_compact")
         return Column(out, arena)
 
+    def slice(self, row_begin: int, row_end: int, carry_in: np.ndarray | None = None) -> "Column":
+        """A view of rows [row_begin, row_end) sharing this column's storage
+        (one rank's shard); carry_in: the 8 lane values before row_begin of a
+        delta_f column (uploaded into the arena), None = zeros."""
+        d_carry = None
+        if carry_in is not None:
+            d_carry = self.arena.alloc(64)
+            _memcpy_h2d(d_carry, np.asarray(carry_in, dtype=np.uint64).reshape(8))
+        out = MsCol()
+        _check(_lib.ms_gpu_col_slice(C.byref(self.desc), row_begin, row_end, d_carry, C.byref(out)), "col_slice")
+        return Column(out, self.arena, keep=self)
+
+    def delta_lane_sums(self, stream=None) -> np.ndarray:
+        """The 8 lane-wise wrapping sums of a delta_f column's deltas."""
+        d = self.arena.alloc(64)
+        _check(_lib.ms_gpu_delta_lane_sums(C.byref(self.desc), d, self.arena.h, _stream_ptr(stream)),
+               "delta_lane_sums")
+        return _memcpy_d2h(d, 64).view(np.uint64).copy()
+
     def build_index(self, stream=None) -> None:
         _check(_lib.ms_gpu_build_index(C.byref(self.desc), self.arena.h, _stream_ptr(stream)), "build_index")
 
@@ -551,6 +574,29 @@ class Batch:
         t = MsTuning()
         _check(_lib.ms_gpu_batch_get_config(self.h, C.byref(t)), "batch_get_config")
         return {"warps": t.warps, "stages": t.stages, "stage_bytes": t.stage_bytes, "ctas_per_sm": t.ctas_per_sm}
+
+    KINDS = {"vbp": 0, "for": 1, "delta": 2, "rest": 3, "rle": 4}
+
+    def set_kind_config(self, kind: str, warps: int | None = None, stages: int = 2, stage_bytes: int = 8192,
+                        ctas_per_sm: int = 1) -> None:
+        """Give one decoder kind ("vbp", "for", "delta", "rest", "rle") its own
+        launch configuration; warps=None returns it to the plan's."""
+        t = None
+        if warps is not None:
+            t = MsTuning(staged=1, warps=warps, stages=stages, stage_bytes=stage_bytes, ctas_per_sm=ctas_per_sm,
+                         values_per_thread=16)
+        _check(_lib.ms_gpu_batch_set_kind_config(self.h, self.KINDS[kind], C.byref(t) if t else None),
+               "batch_set_kind_config")
+
+    def kind_configs(self) -> dict:
+        out = {}
+        for name, k in self.KINDS.items():
+            t, n = MsTuning(), _U64()
+            _check(_lib.ms_gpu_batch_get_kind_config(self.h, k, C.byref(t), C.byref(n)), "batch_get_kind_config")
+            if n.value:
+                out[name] = {"warps": t.warps, "stages": t.stages, "stage_bytes": t.stage_bytes,
+                             "ctas_per_sm": t.ctas_per_sm, "items": int(n.value)}
+        return out
 
     def launch(self, graph: bool = False, stream=None) -> None:
         f = _lib.ms_gpu_batch_run_graph if graph else _lib.ms_gpu_batch_run

@@ -16,7 +16,11 @@ the selected values:
 Both are checked against torch on the uncompressed columns (count and sum
 per column).  GB/s counts the compressed bytes of all columns.
 
-    python -m engine_b200.batch_bench [n_columns] [steps] [--tune] [--no-per-column]
+    python -m engine_b200.batch_bench [n_columns] [steps] [--tune] [--kinds] [--no-per-column]
+
+--kinds also runs one batch per format (the same columns, grouped by kind),
+times each under the global configuration and under every candidate, and
+stores each kind's best as "batch:<kind>/<sm count>" in tuning.json.
 """
 from __future__ import annotations
 
@@ -131,20 +135,82 @@ def load_tuning(ms):
         return None
 
 
-def save_tuning(ms, cfg):
+# benchmark kinds -> the plan's decoder kinds (static_vbp and dynamic_vbp share the vbp decoder)
+DECODER_OF = {"static": "vbp", "dvbp": "vbp", "for": "for", "delta": "delta", "rle": "rle"}
+
+
+def apply_kind_tuning(ms, batch) -> dict:
+    """Per-kind configurations stored by --kinds ("batch:<kind>/<sm>"), where
+    one differs from the plan's; returns the decoder kinds set."""
+    try:
+        with open(os.path.join(HERE, "tuning.json")) as f:
+            d = json.load(f)
+    except (OSError, ValueError):
+        return {}
+    sm = ms.device_info()[0]
+    glob = batch.get_config()
+    applied = {}
+    for kind, dec in DECODER_OF.items():
+        cfg = d.get("batch:%s/%d" % (kind, sm))
+        if not cfg or dec in applied:
+            continue
+        cfg = {k: cfg[k] for k in _CFG_KEYS}
+        if cfg != {k: glob[k] for k in _CFG_KEYS}:
+            batch.set_kind_config(dec, **cfg)
+            applied[dec] = cfg
+    return applied
+
+
+def save_tuning(ms, cfg, key=None):
     path = os.path.join(HERE, "tuning.json")
     try:
         with open(path) as f:
             d = json.load(f)
     except (OSError, ValueError):
         d = {}
-    d[_tuning_key(ms)] = {k: cfg[k] for k in _CFG_KEYS}
+    d[key or _tuning_key(ms)] = {k: cfg[k] for k in _CFG_KEYS}
     with open(path, "w") as f:
         json.dump(d, f, indent=1, sort_keys=True)
 
 
+def time_graph(batch, stream, reps=5) -> float:
+    import torch
+    batch.launch(graph=True, stream=stream)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        batch.launch(graph=True, stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def per_kind(ms, arena, cols, meds, plan, global_cfg, stream) -> dict:
+    """One batch per kind: bytes, GB/s under the global configuration, the
+    best configuration of the sweep and its GB/s."""
+    out = {}
+    for kind in KINDS:
+        idx = [i for i, p in enumerate(plan) if p[1] == kind]
+        if not idx:
+            continue
+        sub = ms.Batch([cols[i] for i in idx], [meds[i] for i in idx], ms.less, arena=arena, stream=stream)
+        try:
+            nbytes = sum(cols[i].get_size_used_byte() for i in idx)
+            sub.set_config(**{k: global_cfg[k] for k in _CFG_KEYS})
+            t_glob = time_graph(sub, stream)
+            best, _ = tune(sub, stream)
+            out[kind] = {"columns": len(idx), "compressed_bytes": nbytes,
+                         "global_cfg_gbs": round(nbytes / (t_glob * 1e-3) / 1e9, 1),
+                         "best": {k: best[k] for k in _CFG_KEYS},
+                         "best_gbs": round(nbytes / (best["ms"] * 1e-3) / 1e9, 1)}
+        finally:
+            sub.close()
+    return out
+
+
 def run(n_cols: int = 4096, steps: int = 10, do_tune: bool = False, per_column_steps: int = 2,
-        per_column: bool = True) -> dict:
+        per_column: bool = True, kinds: bool = False) -> dict:
     import torch
 
     import engine_b200 as ms
@@ -170,6 +236,9 @@ def run(n_cols: int = 4096, steps: int = 10, do_tune: bool = False, per_column_s
             if cfg:
                 batch.set_config(**{k: cfg[k] for k in _CFG_KEYS})
             tuned = dict(batch.get_config(), source="tuning.json" if cfg else "default")
+        if not kinds:
+            apply_kind_tuning(ms, batch)
+        tuned["per_kind"] = batch.kind_configs()
         # batched: graph replay, K steps (events around each replay)
         batch.launch(graph=True, stream=stream)
         batch.launch(graph=True, stream=stream)
@@ -187,6 +256,7 @@ def run(n_cols: int = 4096, steps: int = 10, do_tune: bool = False, per_column_s
         cnt, sm = batch.results()
         ok_b = ok_b and bool(np.array_equal(cnt, e_cnt) and np.array_equal(sm, e_sum))
         info = batch.info()
+        kind_res = per_kind(ms, arena, cols, meds, plan, batch.get_config(), stream) if kinds else None
         batch.close()
         out = {
             "workload": "%d columns, log-uniform lengths 2^10..2^24 (%d rows), formats %s; decompress -> "
@@ -200,6 +270,8 @@ def run(n_cols: int = 4096, steps: int = 10, do_tune: bool = False, per_column_s
             "setup_s": {"generate_and_compress": round(t_build, 2), "plan": round(t_plan, 3)},
             "sweep": swept,
         }
+        if kind_res is not None:
+            out["per_kind"] = kind_res
         if not per_column:
             return out
         # one operator call per column, through the public API
@@ -248,10 +320,15 @@ def main():
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
     n_cols = int(args[0]) if args else 4096
     steps = int(args[1]) if len(args) > 1 else 10
-    r = run(n_cols, steps, do_tune="--tune" in sys.argv, per_column="--no-per-column" not in sys.argv)
+    r = run(n_cols, steps, do_tune="--tune" in sys.argv, per_column="--no-per-column" not in sys.argv,
+            kinds="--kinds" in sys.argv)
     if "--tune" in sys.argv and r["bit_exact"]:
         import engine_b200 as ms
         save_tuning(ms, r["launch"])
+    if r.get("per_kind") and r["bit_exact"]:
+        import engine_b200 as ms
+        for kind, v in r["per_kind"].items():
+            save_tuning(ms, v["best"], key="batch:%s/%d" % (kind, ms.device_info()[0]))
     print(json.dumps(r), flush=True)
     return 0 if r["bit_exact"] else 1
 

@@ -484,14 +484,22 @@ __global__ void k_rle_item_rows(const uint64_t *__restrict__ pairs, uint64_t run
 
 using namespace ms;
 
+constexpr int kBatchKinds = 5;  // kItVbp, kItFor, kItDelta, kItRest, kItRle
+
 struct ms_batch {
     ms_arena *arena;
     uint64_t n_cols, n_items, plan_bytes;
     BCol *d_cols;
     BItem *d_items;
     uint64_t *d_seeks;
-    unsigned long long *d_head;
-    ms_tuning cfg;  // warps, stages, stage_bytes (per warp), ctas_per_sm
+    unsigned long long *d_head;  // one queue head per kind segment
+    ms_tuning cfg;               // warps, stages, stage_bytes (per warp), ctas_per_sm
+    ms_tuning kcfg[kBatchKinds]; // per-kind configuration (kset: set apart from cfg)
+    bool kset[kBatchKinds];
+    uint64_t seg[kBatchKinds + 1];  // items of kind k: [seg[k], seg[k+1]) (the queue is sorted by kind)
+    cudaStream_t side[kBatchKinds];
+    cudaEvent_t fork, join[kBatchKinds];
+    bool streams;
     cudaGraphExec_t graph;
     uint64_t *g_cnt, *g_sum;  // outputs the graph was captured for
 };
@@ -502,22 +510,20 @@ size_t batch_shm(const ms_tuning &t) {
     return size_t(t.warps) * (bwarp_meta_bytes(t.stages) + size_t(t.stages) * t.stage_bytes);
 }
 
-int batch_launch(ms_batch *b, uint64_t *d_cnt, uint64_t *d_sum, cudaStream_t st) {
-    MS_CUDA_TRY(cudaMemsetAsync(b->d_head, 0, 8, st));
-    if (!b->n_cols) return MS_OK;
-    MS_CUDA_TRY(cudaMemsetAsync(d_cnt, 0, 8 * b->n_cols, st));
-    MS_CUDA_TRY(cudaMemsetAsync(d_sum, 0, 8 * b->n_cols, st));
-    if (!b->n_items) return MS_OK;
-    const unsigned S = b->cfg.stages, SB = b->cfg.stage_bytes;
-    const size_t shm = batch_shm(b->cfg);
-    const unsigned grid = unsigned(sm_count()) * b->cfg.ctas_per_sm;
-#define MS_B(Wn)                                                                                                \
-    case Wn:                                                                                                    \
-        k_batch<Wn><<<grid, 32 * Wn, shm, st>>>(b->d_cols, b->d_items, b->n_items, b->d_seeks, S, SB, b->d_head, \
-                                                (unsigned long long *)d_cnt, (unsigned long long *)d_sum,        \
-                                                b->arena->d_err);                                               \
+// One persistent launch over items [i0, i1) with configuration t and queue head `head`.
+int batch_launch_range(ms_batch *b, const ms_tuning &t, uint64_t i0, uint64_t i1, unsigned long long *head,
+                       uint64_t *d_cnt, uint64_t *d_sum, cudaStream_t st) {
+    if (i1 <= i0) return MS_OK;
+    const unsigned S = t.stages, SB = t.stage_bytes;
+    const size_t shm = batch_shm(t);
+    const unsigned grid = unsigned(sm_count()) * t.ctas_per_sm;
+#define MS_B(Wn)                                                                                                 \
+    case Wn:                                                                                                     \
+        k_batch<Wn><<<grid, 32 * Wn, shm, st>>>(b->d_cols, b->d_items + i0, i1 - i0, b->d_seeks, S, SB, head,    \
+                                                (unsigned long long *)d_cnt, (unsigned long long *)d_sum,         \
+                                                b->arena->d_err);                                                \
         break;
-    switch (b->cfg.warps) {
+    switch (t.warps) {
         MS_B(4) MS_B(8) MS_B(12) MS_B(16)
     default: return ms_fail(MS_ERR_INVALID, "batch: warps must be 4, 8, 12 or 16");
     }
@@ -526,8 +532,54 @@ int batch_launch(ms_batch *b, uint64_t *d_cnt, uint64_t *d_sum, cudaStream_t st)
     return MS_OK;
 }
 
-int batch_set_attr(const ms_tuning &t) {
-    const size_t shm = batch_shm(t);
+const ms_tuning &kind_cfg(const ms_batch *b, int k) { return b->kset[k] ? b->kcfg[k] : b->cfg; }
+
+bool same_cfg(const ms_tuning &x, const ms_tuning &y) {
+    return x.warps == y.warps && x.stages == y.stages && x.stage_bytes == y.stage_bytes &&
+           x.ctas_per_sm == y.ctas_per_sm;
+}
+
+int batch_launch(ms_batch *b, uint64_t *d_cnt, uint64_t *d_sum, cudaStream_t st) {
+    MS_CUDA_TRY(cudaMemsetAsync(b->d_head, 0, 8 * kBatchKinds, st));
+    if (!b->n_cols) return MS_OK;
+    MS_CUDA_TRY(cudaMemsetAsync(d_cnt, 0, 8 * b->n_cols, st));
+    MS_CUDA_TRY(cudaMemsetAsync(d_sum, 0, 8 * b->n_cols, st));
+    if (!b->n_items) return MS_OK;
+    bool any = false;
+    for (int k = 0; k < kBatchKinds; k++) any |= b->kset[k] && b->seg[k + 1] > b->seg[k];
+    if (!any) return batch_launch_range(b, b->cfg, 0, b->n_items, b->d_head, d_cnt, d_sum, st);
+    // kind segments with their own configuration: consecutive segments of one
+    // configuration share a launch; the launches run on forked streams, so
+    // one's tail overlaps the next one's start (the joins bring them back)
+    if (!b->streams) {
+        MS_CUDA_TRY(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+        for (int k = 0; k < kBatchKinds; k++) {
+            MS_CUDA_TRY(cudaStreamCreateWithFlags(&b->side[k], cudaStreamNonBlocking));
+            MS_CUDA_TRY(cudaEventCreateWithFlags(&b->join[k], cudaEventDisableTiming));
+        }
+        b->streams = true;
+    }
+    MS_CUDA_TRY(cudaEventRecord(b->fork, st));
+    int g = 0;
+    for (int k = 0; k < kBatchKinds;) {
+        int e = k + 1;
+        while (e < kBatchKinds && same_cfg(kind_cfg(b, e), kind_cfg(b, k))) e++;
+        if (b->seg[e] > b->seg[k]) {
+            MS_CUDA_TRY(cudaStreamWaitEvent(b->side[g], b->fork, 0));
+            const int rc = batch_launch_range(b, kind_cfg(b, k), b->seg[k], b->seg[e], b->d_head + g, d_cnt, d_sum,
+                                              b->side[g]);
+            if (rc) return rc;
+            MS_CUDA_TRY(cudaEventRecord(b->join[g], b->side[g]));
+            MS_CUDA_TRY(cudaStreamWaitEvent(st, b->join[g], 0));
+            g++;
+        }
+        k = e;
+    }
+    return MS_OK;
+}
+
+int batch_set_attr(const ms_tuning &t, size_t at_least = 0) {
+    const size_t shm = batch_shm(t) > at_least ? batch_shm(t) : at_least;
     int dev = 0, maxb = 0, maxsm = 0;
     MS_CUDA_TRY(cudaGetDevice(&dev));
     MS_CUDA_TRY(cudaDeviceGetAttribute(&maxb, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
@@ -546,7 +598,42 @@ int batch_set_attr(const ms_tuning &t) {
     return MS_OK;
 }
 
+// The dynamic shared-memory attribute of every kernel variant: the largest
+// need among the configurations that use it.
+int batch_set_attrs(const ms_batch *b) {
+    for (int w = 4; w <= 16; w += 4) {
+        size_t need = 0;
+        const ms_tuning *use = nullptr;
+        auto consider = [&](const ms_tuning &t) {
+            if (int(t.warps) == w && batch_shm(t) >= need) {
+                need = batch_shm(t);
+                use = &t;
+            }
+        };
+        consider(b->cfg);
+        for (int k = 0; k < kBatchKinds; k++)
+            if (b->kset[k]) consider(b->kcfg[k]);
+        if (use) {
+            const int rc = batch_set_attr(*use, need);
+            if (rc) return rc;
+        }
+    }
+    return MS_OK;
+}
+
+void batch_release(ms_batch *b) {
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    if (b->streams) {
+        cudaEventDestroy(b->fork);
+        for (int k = 0; k < kBatchKinds; k++) {
+            cudaStreamDestroy(b->side[k]);
+            cudaEventDestroy(b->join[k]);
+        }
+    }
+}
+
 int batch_fail(ms_batch *b, int rc) {
+    batch_release(b);
     delete b;
     return rc;
 }
@@ -583,6 +670,8 @@ extern "C" int ms_gpu_batch_create(const ms_col *cols, const uint64_t *consts, u
             hc[i] = b;
             continue;
         }
+        if (c.format == MS_FMT_DELTA_DVBP && c.index_aux)
+            return ms_fail(MS_ERR_UNSUPPORTED, "batch_create: delta_f views with a carry-in are not batched");
         ColView v;
         const uint64_t mark = a->used;
         const bool had_index = c.format == MS_FMT_STATIC_VBP || c.format == MS_FMT_UNCOMPR ||
@@ -620,7 +709,7 @@ extern "C" int ms_gpu_batch_create(const ms_col *cols, const uint64_t *consts, u
     b->d_cols = arena_take_t<BCol>(a, n_cols + 1);
     b->d_items = arena_take_t<BItem>(a, hi.size() + 1);
     b->d_seeks = arena_take_t<uint64_t>(a, 8 * n_seek + 8);
-    b->d_head = arena_take_t<unsigned long long>(a, 1);
+    b->d_head = arena_take_t<unsigned long long>(a, kBatchKinds);
     if (!b->d_cols || !b->d_items || !b->d_seeks || !b->d_head)
         return batch_fail(b, ms_fail(MS_ERR_NOMEM, "arena exhausted (batch plan)"));
     b->plan_bytes = sizeof(BCol) * n_cols + sizeof(BItem) * hi.size() + 64 * n_seek;
@@ -675,6 +764,11 @@ extern "C" int ms_gpu_batch_create(const ms_col *cols, const uint64_t *consts, u
             return kx < ky;
         });
     }
+    // kind segments of the sorted queue
+    for (int k = 0, i = 0; k <= kBatchKinds; k++) {
+        while (i < int(hi.size()) && int(hi[i].kind) < k) i++;
+        b->seg[k] = k == kBatchKinds ? hi.size() : uint64_t(i);
+    }
     if (!hi.empty())
         MS_CUDA_TRY(cudaMemcpyAsync(b->d_items, hi.data(), sizeof(BItem) * hi.size(), cudaMemcpyHostToDevice, st));
     MS_CUDA_TRY(cudaStreamSynchronize(st));
@@ -692,13 +786,51 @@ extern "C" int ms_gpu_batch_set_config(ms_batch *b, const ms_tuning *t) {
         t->ctas_per_sm > 4)
         return ms_fail(MS_ERR_INVALID,
                        "batch_set_config: stages 2..8, stage_bytes >= 4096 (multiple of 128), ctas_per_sm 1..4");
-    int rc = batch_set_attr(*t);
-    if (rc) return rc;
+    if (t->warps < 4 || t->warps > 16 || t->warps % 4)
+        return ms_fail(MS_ERR_INVALID, "batch: warps must be 4, 8, 12 or 16");
+    const ms_tuning prev = b->cfg;
     b->cfg = *t;
+    int rc = batch_set_attrs(b);
+    if (rc) {
+        b->cfg = prev;
+        return rc;
+    }
     if (b->graph) {
         cudaGraphExecDestroy(b->graph);
         b->graph = nullptr;
     }
+    return MS_OK;
+}
+
+extern "C" int ms_gpu_batch_set_kind_config(ms_batch *b, int kind, const ms_tuning *t) {
+    if (!b || kind < 0 || kind >= kBatchKinds) return ms_fail(MS_ERR_INVALID, "batch_set_kind_config: bad argument");
+    if (t && (t->stages < 2 || t->stages > 8 || t->stage_bytes < 4096 || t->stage_bytes % 128 ||
+              t->ctas_per_sm < 1 || t->ctas_per_sm > 4))
+        return ms_fail(MS_ERR_INVALID,
+                       "batch_set_kind_config: stages 2..8, stage_bytes >= 4096 (multiple of 128), ctas_per_sm 1..4");
+    if (t && (t->warps < 4 || t->warps > 16 || t->warps % 4))
+        return ms_fail(MS_ERR_INVALID, "batch: warps must be 4, 8, 12 or 16");
+    const ms_tuning prev = b->kcfg[kind];
+    const bool prev_set = b->kset[kind];
+    b->kset[kind] = t != nullptr;
+    if (t) b->kcfg[kind] = *t;
+    int rc = batch_set_attrs(b);
+    if (rc) {
+        b->kcfg[kind] = prev;
+        b->kset[kind] = prev_set;
+        return rc;
+    }
+    if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    return MS_OK;
+}
+
+extern "C" int ms_gpu_batch_get_kind_config(const ms_batch *b, int kind, ms_tuning *t, uint64_t *n_items) {
+    if (!b || !t || kind < 0 || kind >= kBatchKinds) return ms_fail(MS_ERR_INVALID, "batch_get_kind_config");
+    *t = b->kset[kind] ? b->kcfg[kind] : b->cfg;
+    if (n_items) *n_items = b->seg[kind + 1] - b->seg[kind];
     return MS_OK;
 }
 
@@ -752,6 +884,6 @@ extern "C" int ms_gpu_batch_info(const ms_batch *b, uint64_t *n_items, uint64_t 
 
 extern "C" void ms_gpu_batch_destroy(ms_batch *b) {
     if (!b) return;
-    if (b->graph) cudaGraphExecDestroy(b->graph);
+    batch_release(b);
     delete b;
 }

@@ -545,12 +545,13 @@ namespace ms {
 // takes slots 32h..32h+31 of lane l (word-aligned half streams); wider
 // blocks fall back to the 16-value form on quarters 2h and 2h+1.
 // Threshold select + sum of the same 32 values on top-aligned fields: the
-// test is `top < T * 2^(32-BW)` (see vbp_lt32_top) and the value is
-// `top >> (32-BW)`, so no mask word is built and re-read: a shift, a
-// compare and two predicated adds per value.
-template <unsigned BW>
+// test is `top < T * 2^(32-BW)` (see vbp_lt32_top), the value
+// `top >> (32-BW)`; the hit becomes a 0/1 flag that multiplies the value into
+// the sum and adds to the count (integer multiply-adds instead of predicated
+// adds on the ALU).
+template <unsigned BW, bool kFlip>
 __device__ __forceinline__ uint64_t vbp_ltsum32_top(const uint64_t *__restrict__ blk, unsigned l, unsigned h,
-                                                    uint32_t T, bool flip, unsigned &cnt) {
+                                                    uint32_t T, unsigned &cnt) {
     static_assert(BW <= 32, "32-bit fields");
     constexpr unsigned NW = (32 * BW + 63) / 64 + 1;
     constexpr unsigned NH = BW + 1;
@@ -571,30 +572,34 @@ __device__ __forceinline__ uint64_t vbp_ltsum32_top(const uint64_t *__restrict__
         else n[i] = (i + 1 < 2 * NW) ? (o ? hw[i + 1] : hw[i]) : ((i < 2 * NW && !o) ? hw[i] : 0);
     }
     const uint32_t Tt = BW == 32 ? T : (T << (32u - BW));
-    unsigned c = 0;
+    uint32_t c0 = 0, c1 = 0, s0 = 0, s1 = 0;
     uint64_t s64 = 0;
-    uint32_t s32 = 0;
 #pragma unroll
     for (unsigned k = 0; k < 32; k++) {
         const unsigned p = k * BW, wi = p >> 5, sh = p & 31u;
         const uint32_t top = (sh + BW <= 32) ? (n[wi] << (32u - sh - BW)) : __funnelshift_r(n[wi], n[wi + 1], sh + BW - 32u);
-        const bool hit = (top < Tt) != flip;
+        const bool lt = top < Tt;
+        const uint32_t f = (kFlip ? !lt : lt) ? 1u : 0u;
         const uint32_t v = BW == 32 ? top : (top >> (32u - BW));
-        if (hit) {
-            c++;
-            if (BW <= 26) s32 += v;  // 32 values of < 2^26 fit a 32-bit partial sum
-            else s64 += v;
+        if (k & 1) c1 += f;
+        else c0 += f;
+        if (BW <= 26) {  // 32 values of < 2^26 fit a 32-bit partial sum
+            if (k & 1) s1 += v * f;
+            else s0 += v * f;
+        } else {
+            s64 += uint64_t(v) * f;
         }
     }
-    cnt = c;
-    return BW <= 26 ? uint64_t(s32) : s64;
+    cnt = c0 + c1;
+    return BW <= 26 ? uint64_t(s0) + s1 : s64;
 }
 
 template <unsigned BW>
 __device__ __forceinline__ uint64_t self_sum32_block(const uint64_t *blk, unsigned l, unsigned h, const Pred &p,
                                                      unsigned &cnt) {
     if (BW <= 32 && !p.is_eq && p.T < (uint64_t(1) << (BW <= 32 ? BW : 32))) {
-        return vbp_ltsum32_top<(BW <= 32 ? BW : 32)>(blk, l, h, uint32_t(p.T), p.flip != 0, cnt);
+        return p.flip ? vbp_ltsum32_top<(BW <= 32 ? BW : 32), true>(blk, l, h, uint32_t(p.T), cnt)
+                      : vbp_ltsum32_top<(BW <= 32 ? BW : 32), false>(blk, l, h, uint32_t(p.T), cnt);
     } else if (BW <= 32) {
         uint32_t v[32];
         vbp_decode32_u32<(BW <= 32 ? BW : 32)>(blk, l, h, v);

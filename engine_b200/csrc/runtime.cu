@@ -23,7 +23,7 @@ int ms_fail(int status, const char *what) {
 
 extern "C" int ms_gpu_abi_version(void) { return MS_ABI_VERSION; }
 
-static ms_tuning g_tuning = {1, 24, 4, 49152, 1, 16};
+static ms_tuning g_tuning = {1, 16, 3, 65536, 1, 32};  // the tuned headline configuration
 
 ms_tuning ms::tuning() { return g_tuning; }
 
@@ -334,6 +334,13 @@ __global__ void __launch_bounds__(256) k_delta_block_sums(ms::ColView c, uint64_
 
 }  // namespace
 
+// A delta_f view's carry-in (the 8 lane values before its first row) added
+// to every block's lane carry.
+__global__ void k_add_carry_in(uint64_t *__restrict__ carry, uint64_t nb, const uint64_t *__restrict__ carry_in) {
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nb * 8; i += uint64_t(gridDim.x) * blockDim.x)
+        carry[i] += carry_in[i & 7];
+}
+
 int ms::build_index_device(const ms_col *c, uint64_t *index, uint64_t *aux, unsigned *d_err, cudaStream_t st) {
     const uint64_t ncompr = c->count_values - count_rest(*c);
     const uint64_t nb = ncompr / kBlock;
@@ -361,14 +368,16 @@ extern "C" int ms_gpu_col_compact(const ms_col *in, ms_col *out, ms_arena *a, vo
     cudaStream_t st = (cudaStream_t)stream;
     const uint64_t bytes = in->size_used_byte;
     const bool has_index = in->index && in->n_index, has_aux = in->index_aux && in->n_index;
+    // index_aux: FOR references (one per 1024 rows) or a delta_f view's 8 carry-in lanes
+    const uint64_t aux_words = in->format == MS_FMT_DELTA_DVBP ? 8 : in->n_index / 2;
     uint8_t *data = arena_take_t<uint8_t>(a, bytes + 64);
     uint64_t *index = has_index ? arena_take_t<uint64_t>(a, in->n_index + 1) : nullptr;
-    uint64_t *aux = has_aux ? arena_take_t<uint64_t>(a, in->n_index / 2 + 1) : nullptr;
+    uint64_t *aux = has_aux ? arena_take_t<uint64_t>(a, aux_words + 1) : nullptr;
     if (!data || (has_index && !index) || (has_aux && !aux)) return ms_fail(MS_ERR_NOMEM, "arena exhausted (col_compact)");
     if (bytes) MS_CUDA_TRY(cudaMemcpyAsync(data, in->data, bytes, cudaMemcpyDeviceToDevice, st));
     if (index) MS_CUDA_TRY(cudaMemcpyAsync(index, in->index, 8 * in->n_index, cudaMemcpyDeviceToDevice, st));
-    if (aux && in->n_index / 2)
-        MS_CUDA_TRY(cudaMemcpyAsync(aux, in->index_aux, 8 * (in->n_index / 2), cudaMemcpyDeviceToDevice, st));
+    if (aux && aux_words)
+        MS_CUDA_TRY(cudaMemcpyAsync(aux, in->index_aux, 8 * aux_words, cudaMemcpyDeviceToDevice, st));
     ms_col c = *in;
     c.data = data;
     c.size_alloc_byte = bytes + 64;
@@ -571,8 +580,96 @@ int ms::prepare_view(const ms_col *c, ms_arena *a, cudaStream_t st, ColView *v) 
         k_delta_block_sums<<<persistent_grid(256, 8), 256, 0, st>>>(w, sums, a->d_err);
         MS_CUDA_TRY(cudaGetLastError());
         MS_CUDA_TRY((scan_exclusive<uint64_t, 8>(sums, nb, carry, tot, scr, st)));
+        if (c->index_aux) {  // a view's carry-in
+            k_add_carry_in<<<unsigned(minu((nb * 8 + 255) / 256, uint64_t(persistent_grid(256, 4)))), 256, 0, st>>>(
+                carry, nb, c->index_aux);
+            MS_CUDA_TRY(cudaGetLastError());
+        }
         w.carry = carry;
     }
     *v = w;
     return MS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Views of block ranges (one rank's shard of a column) and the delta_f
+// lane sums a shard hands to the next one
+// ---------------------------------------------------------------------------
+extern "C" int ms_gpu_col_slice(const ms_col *in, uint64_t row_begin, uint64_t row_end, const uint64_t *d_carry_in,
+                                ms_col *out) {
+    using namespace ms;
+    if (!in || !out) return ms_fail(MS_ERR_INVALID, "col_slice: null argument");
+    int rc = check_col(in, false);
+    if (rc) return rc;
+    const int fmt = int(in->format);
+    const uint64_t n = in->count_values;
+    if (row_begin > row_end || row_end > n) return ms_fail(MS_ERR_INVALID, "col_slice: rows outside the column");
+    if (fmt == MS_FMT_RLE) return ms_fail(MS_ERR_UNSUPPORTED, "col_slice: rle_f has no block structure");
+    if (d_carry_in && fmt != MS_FMT_DELTA_DVBP) return ms_fail(MS_ERR_INVALID, "col_slice: a carry-in is for delta_f");
+    if (fmt == MS_FMT_DELTA_DVBP && in->index_aux)
+        return ms_fail(MS_ERR_UNSUPPORTED, "col_slice: a delta_f view with a carry-in cannot be sliced again");
+    ms_col v = *in;
+    v.count_values = row_end - row_begin;
+    if (fmt == MS_FMT_UNCOMPR) {
+        if (row_begin % 2) return ms_fail(MS_ERR_INVALID, "col_slice: uncompr_f views start at an even row");
+        v.data = static_cast<uint8_t *>(in->data) + 8 * row_begin;
+        v.size_used_byte = v.size_alloc_byte = 8 * v.count_values;
+        v.size_compr_byte = 0;
+        *out = v;
+        return MS_OK;
+    }
+    const uint64_t nrest = count_rest(*in), ncompr = n - nrest, unit = block_size(fmt);
+    const bool last = row_end == n;
+    if (row_begin % unit || row_begin > ncompr)
+        return ms_fail(MS_ERR_INVALID, "col_slice: a view starts on a block boundary of the compressed part");
+    if (!last && (row_end % unit || row_end > ncompr))
+        return ms_fail(MS_ERR_INVALID, "col_slice: a view ends on a block boundary or at the column's end");
+    const uint64_t b0 = row_begin / kBlock, b1 = (last ? ncompr : row_end) / kBlock;
+    if (fmt == MS_FMT_STATIC_VBP) {
+        const uint64_t boff = b0 * 64 * in->bw;
+        v.data = static_cast<uint8_t *>(in->data) + boff;
+        v.size_compr_byte = (b1 - b0) * 64 * in->bw;
+        v.size_used_byte = last && nrest ? rest_offset(fmt, in->bw, v.size_compr_byte) + 8 * nrest : v.size_compr_byte;
+        v.size_alloc_byte = in->size_alloc_byte - boff;
+        v.index = v.index_aux = nullptr;
+        v.n_index = 0;
+    } else {
+        if (b1 > b0 && (!in->index || in->n_index < b1 || (fmt == MS_FMT_FOR_DVBP && !in->index_aux)))
+            return ms_fail(MS_ERR_INVALID, "col_slice: the column needs its block index (ms_gpu_build_index)");
+        // blocks are found through the index (offsets from the column's start);
+        // the sizes only place the uncompressed rest, which the last view keeps
+        v.index = in->index ? in->index + b0 : nullptr;
+        v.n_index = b1 - b0;
+        v.index_aux = fmt == MS_FMT_FOR_DVBP ? (in->index_aux ? in->index_aux + b0 / 2 : nullptr)
+                      : fmt == MS_FMT_DELTA_DVBP ? const_cast<uint64_t *>(d_carry_in)
+                                                 : nullptr;
+        if (!last) v.size_used_byte = v.size_compr_byte;
+    }
+    *out = v;
+    return MS_OK;
+}
+
+extern "C" int ms_gpu_delta_lane_sums(const ms_col *in, uint64_t *d_sums, ms_arena *a, void *stream) {
+    using namespace ms;
+    if (!in || !d_sums || !a) return ms_fail(MS_ERR_INVALID, "delta_lane_sums: null argument");
+    if (in->format != MS_FMT_DELTA_DVBP) return ms_fail(MS_ERR_INVALID, "delta_lane_sums: not a delta_f column");
+    cudaStream_t st = (cudaStream_t)stream;
+    ColView w;
+    ms_col c = *in;
+    c.index_aux = nullptr;  // the sums do not depend on the carry-in
+    int rc = prepare_view(&c, a, st, &w);
+    if (rc) return rc;
+    const uint64_t nb = w.nb();
+    if (!nb) {
+        MS_CUDA_TRY(cudaMemsetAsync(d_sums, 0, 8 * sizeof(uint64_t), st));
+        return MS_OK;
+    }
+    uint64_t *sums = arena_take_t<uint64_t>(a, nb * 8);
+    uint64_t *excl = arena_take_t<uint64_t>(a, nb * 8);
+    uint64_t *scr = arena_take_t<uint64_t>(a, scan_scratch_words(nb, 8));
+    if (!sums || !excl || !scr) return ms_fail(MS_ERR_NOMEM, "arena exhausted (delta lane sums)");
+    k_delta_block_sums<<<persistent_grid(256, 8), 256, 0, st>>>(w, sums, a->d_err);
+    MS_CUDA_TRY(cudaGetLastError());
+    MS_CUDA_TRY((scan_exclusive<uint64_t, 8>(sums, nb, excl, d_sums, scr, st)));
+    return read_err(a, st);
 }

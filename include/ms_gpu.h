@@ -150,6 +150,29 @@ int ms_gpu_build_index(ms_col *col, ms_arena *arena, void *stream);
  * can be compacted after it is produced.  Asynchronous. */
 int ms_gpu_col_compact(const ms_col *in, ms_col *out, ms_arena *arena, void *stream);
 
+/* Views of block ranges, for sharding one column across ranks (no
+ * counterpart in the reference, whose columns are never split).  A view of
+ * rows [row_begin, row_end) shares the column's storage and block index; no
+ * data is copied and nothing is allocated.  row_begin lies on a block
+ * boundary of the compressed part (512 rows; 1024 for delta_f and for_f; an
+ * even row for uncompr_f) and so does row_end, unless it is the column's
+ * count, in which case the view keeps the uncompressed rest.  Every operator
+ * treats a view as a column of its own (its scalar remainder included).
+ * dynamic_vbp-family columns need their block index.  A delta_f view decodes
+ * from d_carry_in, the 8 lane values of the row before row_begin (device
+ * array; NULL = zeros, as at the column's start), which the view keeps by
+ * reference in out->index_aux; a rank obtains it as the lane-wise sum of the
+ * earlier shards' ms_gpu_delta_lane_sums.  Views are not batched
+ * (ms_gpu_batch_create rejects a delta_f view with a carry-in) and are not
+ * stored: store or compact the column itself. */
+int ms_gpu_col_slice(const ms_col *in, uint64_t row_begin, uint64_t row_end, const uint64_t *d_carry_in,
+                     ms_col *out);
+/* The 8 lane-wise wrapping sums of a delta_f column's (or view's) deltas over
+ * its compressed part (delta.h:229-262 decodes value i as the running sum of
+ * lane i mod 8), written to device d_sums[0..8): what a shard adds to the
+ * carry-in of the shards after it.  Synchronises `stream`. */
+int ms_gpu_delta_lane_sums(const ms_col *in, uint64_t *d_sums, ms_arena *arena, void *stream);
+
 /* ---- persistence (binary_io<F>, include/core/persistence/binary_io.h:40-87)
  * File layout as the reference's: [count_values u64][size_used_byte u64]
  * [size_used_byte bytes of the column buffer].  store copies the column to
@@ -288,6 +311,16 @@ int ms_gpu_batch_create(const ms_col *cols, const uint64_t *consts, uint64_t n_c
  * ctas_per_sm; other fields ignored */
 int ms_gpu_batch_set_config(ms_batch *b, const ms_tuning *t);
 int ms_gpu_batch_get_config(const ms_batch *b, ms_tuning *t);
+/* The queue is sorted by decoder kind: MS_BATCH_VBP (static_vbp and
+ * dynamic_vbp blocks), MS_BATCH_FOR, MS_BATCH_DELTA, MS_BATCH_REST
+ * (uncompressed rows), MS_BATCH_RLE.  A kind may get its own configuration
+ * (t = NULL: back to the plan's); the run then launches consecutive kinds of
+ * one configuration together, each launch on its own forked stream (joined
+ * before the run ends; a graph captures the fork and join).  get also reports
+ * the kind's number of work items. */
+enum { MS_BATCH_VBP = 0, MS_BATCH_FOR = 1, MS_BATCH_DELTA = 2, MS_BATCH_REST = 3, MS_BATCH_RLE = 4 };
+int ms_gpu_batch_set_kind_config(ms_batch *b, int kind, const ms_tuning *t);
+int ms_gpu_batch_get_kind_config(const ms_batch *b, int kind, ms_tuning *t, uint64_t *n_items);
 int ms_gpu_batch_run(ms_batch *b, uint64_t *d_counts, uint64_t *d_sums, void *stream);
 int ms_gpu_batch_run_graph(ms_batch *b, uint64_t *d_counts, uint64_t *d_sums, void *stream);
 int ms_gpu_batch_info(const ms_batch *b, uint64_t *n_items, uint64_t *plan_bytes);

@@ -93,6 +93,41 @@ def test_batch_launch_configs(ms, arena, orc, cfg):
     b.close()
 
 
+@pytest.mark.parametrize("kinds", [{"rle": dict(warps=16, stages=2, stage_bytes=4096)},
+                                   {"delta": dict(warps=16, stages=2, stage_bytes=4096),
+                                    "rle": dict(warps=16, stages=2, stage_bytes=4096)},
+                                   {"vbp": dict(warps=8, stages=3, stage_bytes=8192),
+                                    "for": dict(warps=12, stages=2, stage_bytes=8192),
+                                    "delta": dict(warps=4, stages=4, stage_bytes=4096, ctas_per_sm=2),
+                                    "rest": dict(warps=16, stages=2, stage_bytes=4096),
+                                    "rle": dict(warps=8, stages=2, stage_bytes=4096)}])
+def test_batch_per_kind_configs(ms, arena, orc, kinds):
+    """Kinds with their own launch configuration: one launch per run of
+    equally configured kinds, on forked streams; direct and graph replay
+    give the oracle's counts and sums, and a kind returned to the plan's
+    configuration leaves a single launch."""
+    lengths = _lengths(orc, 40, 10, 17, 11)
+    cols, vals, consts = _make(ms, arena, orc, lengths, seed0=6)
+    b = ms.Batch(cols, consts)
+    b.set_config(warps=12, stages=2, stage_bytes=8192)
+    for k, cfg in kinds.items():
+        b.set_kind_config(k, **cfg)
+    got = b.kind_configs()
+    for k, cfg in kinds.items():
+        if k in got:
+            assert {x: got[k][x] for x in ("warps", "stages", "stage_bytes", "ctas_per_sm")} == \
+                dict(dict(ctas_per_sm=1), **cfg)
+    for graph in (False, True, True):
+        cnt, s = b.run(graph=graph)
+        for i, (v, c) in enumerate(zip(vals, consts)):
+            assert (int(cnt[i]), int(s[i])) == _expect(orc, v, c), (i, kinds)
+    for k in kinds:
+        b.set_kind_config(k, None)
+    cnt2, s2 = b.run(graph=True)
+    assert np.array_equal(cnt2, cnt) and np.array_equal(s2, s)
+    b.close()
+
+
 @pytest.mark.parametrize("cmp", [O.CMP_EQ, O.CMP_LE, O.CMP_GT, O.CMP_GE])
 def test_batch_other_comparisons(ms, arena, orc, cmp):
     lengths = _lengths(orc, 15, 10, 14, 30 + cmp)
