@@ -402,15 +402,25 @@ __global__ void __launch_bounds__(kRleEncThreads) k_rle_encode(const uint64_t *_
 
 constexpr unsigned kRleThreads = 256;
 constexpr unsigned kRleRunsPerThread = 8;
-constexpr unsigned kRleTile = kRleThreads * kRleRunsPerThread;  // runs per decoder tile
+constexpr unsigned kRleTile = kRleThreads * kRleRunsPerThread;  // most runs per decoder tile
+constexpr unsigned kRleRows = 8192;  // output rows per decoder CTA
+// Runs per decoder tile: about as many as one output chunk of kRleRows rows
+// holds at the column's mean run length, a power of two in [kRleThreads,
+// kRleTile].  Long runs thus mean small tiles, so a chunk loads and scans
+// few runs it does not write.
+inline unsigned rle_tile_runs(uint64_t n, uint64_t runs) {
+    unsigned tr = kRleTile;
+    while (tr > kRleThreads && uint64_t(tr) * n > uint64_t(kRleRows) * runs) tr >>= 1;
+    return tr;
+}
 
 // Decoder, pass 1: run lengths summed per tile of kRleTile runs.
 __global__ void __launch_bounds__(kRleThreads) k_rle_tile_rows(const uint64_t *__restrict__ pairs, uint64_t runs,
-                                                              uint64_t *__restrict__ tile_rows) {
+                                                              unsigned tr, uint64_t *__restrict__ tile_rows) {
     __shared__ uint64_t s_w[kRleThreads / 32];
-    const uint64_t t = blockIdx.x, base = t * kRleTile;
+    const uint64_t t = blockIdx.x, base = t * tr;
     uint64_t s = 0;
-    for (unsigned i = threadIdx.x; i < kRleTile; i += kRleThreads) {
+    for (unsigned i = threadIdx.x; i < tr; i += kRleThreads) {
         const uint64_t r = base + i;
         if (r < runs) s += __ldg(pairs + 2 * r + 1);
     }
@@ -428,7 +438,6 @@ __global__ void __launch_bounds__(kRleThreads) k_rle_tile_rows(const uint64_t *_
 // Decoder, pass 2: the run tile holding the first row of every chunk of
 // kRleRows output rows (one thread per chunk, binary search over the tiles'
 // first rows).
-constexpr unsigned kRleRows = 8192;
 
 __global__ void k_rle_chunk_tiles(const uint64_t *__restrict__ tile_first, uint64_t ntiles, uint64_t chunks,
                                   uint32_t *__restrict__ chunk_tile) {
@@ -445,67 +454,129 @@ __global__ void k_rle_chunk_tiles(const uint64_t *__restrict__ tile_first, uint6
 }
 
 // Decoder, pass 3: each CTA writes kRleRows output rows.  Starting at the
-// run tile that holds its first row,
-// loads that tile's values and run starts into shared memory (a scan of the
-// lengths), writes the rows the tile covers (each row's run by binary search
-// in shared memory) and moves on to the next tile until its rows are done.
+// run tile that holds its first row, it stages that tile's pairs in shared
+// memory and turns them into (value, start) lists -- zero-length runs
+// dropped, as they write nothing (rle.h:238-249) -- while marking each run
+// start inside its rows in a bitmap (one 32-bit word per 32 rows).  Each
+// warp then writes a contiguous range of words: row 32 u + l belongs to the
+// run counted by the starts before word u plus the bits of word u at or
+// below l.  It moves on to the next tile until its rows are done.  RPT runs
+// per thread: the tile holds RPT * kRleThreads runs.
+template <unsigned RPT>
 __global__ void __launch_bounds__(kRleThreads) k_rle_expand(const uint64_t *__restrict__ pairs, uint64_t runs,
                                                            const uint64_t *__restrict__ tile_first, uint64_t ntiles,
                                                            const uint32_t *__restrict__ chunk_tile,
                                                            const uint64_t *__restrict__ total_rows, uint64_t n,
                                                            uint64_t *__restrict__ out, unsigned *err) {
-    __shared__ uint64_t s_val[kRleTile];
-    __shared__ uint64_t s_start[kRleTile];
-    __shared__ uint64_t s_wsum[kRleThreads / 32];
+    constexpr unsigned NWP = kRleThreads / 32, TR = RPT * kRleThreads, NWD = kRleRows / 32;
+    __shared__ uint64_t s_val[TR];
+    __shared__ uint64_t s_len[TR];  // lengths, then (as 32-bit words) the kept runs' entries
+    __shared__ unsigned s_bits[NWD];  // run starts per 32-row word of the CTA's rows
+    __shared__ uint64_t s_wsum[NWP];
+    __shared__ unsigned s_wcnt[NWP];
+    // a kept run's entry is 1 + its start's offset from row0 (0: it starts
+    // before row0): row row0 + r lies in the last run whose entry is <= r + 1
+    uint32_t *const s_st = reinterpret_cast<uint32_t *>(s_len);
     const uint64_t row0 = uint64_t(blockIdx.x) * kRleRows;
     if (row0 >= n) return;
     const uint64_t row1 = minu(n, row0 + kRleRows);
     const unsigned lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+    const unsigned incl = (2u << lane) - 1u;  // lanes 0..lane
     for (uint64_t t = chunk_tile[blockIdx.x]; t < ntiles && tile_first[t] < row1; t++) {
-        const uint64_t rbase = t * kRleTile;
-        const unsigned nr = unsigned(minu(kRleTile, runs - rbase));
+        const uint64_t rbase = t * TR;
+        const unsigned nr = unsigned(minu(TR, runs - rbase));
         // the tile's pairs into shared memory, one 16-byte pair per thread and step
-        for (unsigned j = threadIdx.x; j < kRleTile; j += kRleThreads) {
+#pragma unroll
+        for (unsigned k = 0; k < RPT; k++) {
+            const unsigned j = threadIdx.x + k * kRleThreads;
             const ulonglong2 pr = j < nr ? __ldg(reinterpret_cast<const ulonglong2 *>(pairs) + rbase + j)
                                          : make_ulonglong2(0, 0);
             s_val[j] = pr.x;
-            s_start[j] = pr.y;
+            s_len[j] = pr.y;
         }
+        for (unsigned w = threadIdx.x; w < NWD; w += kRleThreads) s_bits[w] = 0;
         __syncthreads();
-        // this thread's kRleRunsPerThread consecutive runs: an exclusive scan of the lengths
-        const unsigned j0 = threadIdx.x * kRleRunsPerThread;
-        uint64_t len[kRleRunsPerThread], sum = 0;
+        // this thread's RPT consecutive runs: exclusive scans of the lengths
+        // and of the number of non-empty runs
+        const unsigned j0 = threadIdx.x * RPT;
+        uint64_t len[RPT], val[RPT], sum = 0;
+        unsigned cnt = 0;
 #pragma unroll
-        for (unsigned k = 0; k < kRleRunsPerThread; k++) {
-            len[k] = s_start[j0 + k];
+        for (unsigned k = 0; k < RPT; k++) {
+            len[k] = s_len[j0 + k];
+            val[k] = s_val[j0 + k];
             sum += len[k];
+            cnt += len[k] != 0;
         }
-        uint64_t incl = sum;
+        uint64_t isum = sum;
+        unsigned icnt = cnt;
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
-            const uint64_t o = __shfl_up_sync(0xFFFFFFFFu, incl, d);
-            if (int(lane) >= d) incl += o;
+            const uint64_t o = __shfl_up_sync(0xFFFFFFFFu, isum, d);
+            const unsigned co = __shfl_up_sync(0xFFFFFFFFu, icnt, d);
+            if (int(lane) >= d) {
+                isum += o;
+                icnt += co;
+            }
         }
-        if (lane == 31) s_wsum[wid] = incl;
+        if (lane == 31) {
+            s_wsum[wid] = isum;
+            s_wcnt[wid] = icnt;
+        }
         __syncthreads();
-        uint64_t run = tile_first[t] + incl - sum;
-        for (unsigned w = 0; w < wid; w++) run += s_wsum[w];
+        // the warps before this one: lanes 0..NWP-1 scan the warp totals
+        uint64_t ws = lane < NWP ? s_wsum[lane] : 0;
+        unsigned wc = lane < NWP ? s_wcnt[lane] : 0;
 #pragma unroll
-        for (unsigned k = 0; k < kRleRunsPerThread; k++) {
-            s_start[j0 + k] = j0 + k < nr ? run : ~uint64_t(0);
+        for (int d = 1; d < int(NWP); d <<= 1) {
+            const uint64_t o = __shfl_up_sync(0xFFFFFFFFu, ws, d);
+            const unsigned co = __shfl_up_sync(0xFFFFFFFFu, wc, d);
+            if (int(lane) >= d) {
+                ws += o;
+                wc += co;
+            }
+        }
+        const unsigned kept = __shfl_sync(0xFFFFFFFFu, wc, NWP - 1);
+        const uint64_t wpre = wid ? __shfl_sync(0xFFFFFFFFu, ws, wid - 1) : 0;
+        const unsigned cpre = wid ? __shfl_sync(0xFFFFFFFFu, wc, wid - 1) : 0;
+        uint64_t run = tile_first[t] + wpre + isum - sum;
+        unsigned pos = cpre + icnt - cnt;
+#pragma unroll
+        for (unsigned k = 0; k < RPT; k++) {
+            if (len[k]) {
+                const uint32_t e = run < row0 ? 0u : uint32_t(minu(run - row0 + 1, 0xFFFFFFFFull));
+                s_st[pos] = e;
+                s_val[pos] = val[k];
+                if (e - 1u < kRleRows) atomicOr(&s_bits[(e - 1u) >> 5], 1u << ((e - 1u) & 31u));
+                pos++;
+            }
             run += len[k];
         }
         __syncthreads();
         const uint64_t tile_end = t + 1 < ntiles ? tile_first[t + 1] : n;
         const uint64_t a = maxu(row0, tile_first[t]), b = minu(row1, tile_end);
-        for (uint64_t r = a + threadIdx.x; r < b; r += kRleThreads) {
-            unsigned lo = 0, hi = nr;  // last run of the tile with start <= r
-            while (hi - lo > 1) {
-                const unsigned mid = (lo + hi) >> 1;
-                if (s_start[mid] <= r) lo = mid;
-                else hi = mid;
+        if (a < b) {
+            const uint32_t ra = uint32_t(a - row0), rb = uint32_t(b - row0);
+            const uint32_t tw0 = ra >> 5, tw1 = (rb + 31) >> 5;
+            // the words split evenly over the warps
+            const uint32_t per = (tw1 - tw0 + NWP - 1) / NWP;
+            const uint32_t u0 = tw0 + wid * per, u1 = min(tw1, u0 + per);
+            if (u0 < u1) {
+                unsigned lo = 0, hi = kept;  // runs with entry <= 32 u0
+                while (lo < hi) {
+                    const unsigned mid = (lo + hi) >> 1;
+                    if (s_st[mid] > 32 * u0) hi = mid;
+                    else lo = mid + 1;
+                }
+                unsigned before = lo - 1u;  // index of the run holding row 32 u0 - 1 (wraps for none)
+                uint64_t *const o = out + row0 + lane;
+                for (uint32_t u = u0; u < u1; u++) {
+                    const unsigned bits = s_bits[u];
+                    const uint32_t r = 32 * u + lane;
+                    if (r >= ra && r < rb) o[32 * u] = s_val[min(before + __popc(bits & incl), kept - 1)];
+                    before += __popc(bits);
+                }
             }
-            out[r] = s_val[lo];
         }
         __syncthreads();
     }
@@ -550,14 +621,15 @@ static int decode_rle(const ms_col *in, uint64_t *d_out, ms_arena *a, cudaStream
     const uint64_t runs = in->size_used_byte / 16, n = in->count_values;
     if (!n) return MS_OK;
     if (!runs) return ms_fail(MS_ERR_CORRUPT, "rle column with values but no runs");
-    const uint64_t tiles = (runs + kRleTile - 1) / kRleTile;
+    const unsigned tr = rle_tile_runs(n, runs);
+    const uint64_t tiles = (runs + tr - 1) / tr;
     uint64_t *trows = arena_take_t<uint64_t>(a, tiles + 1);
     uint64_t *tfirst = arena_take_t<uint64_t>(a, tiles + 1);
     uint64_t *tot = arena_take_t<uint64_t>(a, 1);
     uint64_t *scr = arena_take_t<uint64_t>(a, scan_scratch_words(tiles, 1));
     if (!trows || !tfirst || !tot || !scr) return ms_fail(MS_ERR_NOMEM, "arena exhausted (rle decode)");
     const uint64_t *pairs = (const uint64_t *)in->data;
-    k_rle_tile_rows<<<unsigned(tiles), kRleThreads, 0, st>>>(pairs, runs, trows);
+    k_rle_tile_rows<<<unsigned(tiles), kRleThreads, 0, st>>>(pairs, runs, tr, trows);
     MS_CUDA_TRY(cudaGetLastError());
     MS_CUDA_TRY((scan_exclusive<uint64_t, 1>(trows, tiles, tfirst, tot, scr, st)));
     const uint64_t chunks = (n + kRleRows - 1) / kRleRows;
@@ -566,7 +638,12 @@ static int decode_rle(const ms_col *in, uint64_t *d_out, ms_arena *a, cudaStream
     k_rle_chunk_tiles<<<unsigned(minu((chunks + 255) / 256, uint64_t(persistent_grid(256, 4)))), 256, 0, st>>>(
         tfirst, tiles, chunks, ctile);
     MS_CUDA_TRY(cudaGetLastError());
-    k_rle_expand<<<unsigned(chunks), kRleThreads, 0, st>>>(pairs, runs, tfirst, tiles, ctile, tot, n, d_out, a->d_err);
+    switch (tr / kRleThreads) {
+    case 1: k_rle_expand<1><<<unsigned(chunks), kRleThreads, 0, st>>>(pairs, runs, tfirst, tiles, ctile, tot, n, d_out, a->d_err); break;
+    case 2: k_rle_expand<2><<<unsigned(chunks), kRleThreads, 0, st>>>(pairs, runs, tfirst, tiles, ctile, tot, n, d_out, a->d_err); break;
+    case 4: k_rle_expand<4><<<unsigned(chunks), kRleThreads, 0, st>>>(pairs, runs, tfirst, tiles, ctile, tot, n, d_out, a->d_err); break;
+    default: k_rle_expand<8><<<unsigned(chunks), kRleThreads, 0, st>>>(pairs, runs, tfirst, tiles, ctile, tot, n, d_out, a->d_err); break;
+    }
     MS_CUDA_TRY(cudaGetLastError());
     return MS_OK;
 }

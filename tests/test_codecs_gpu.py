@@ -141,7 +141,8 @@ def test_compact_keeps_column(ms, arena, orc, fmt):
 
 
 def _rle_cases(orc):
-    t = 2048  # the encoder's tile of rows
+    t = 2048  # the decoder's largest tile of runs
+    T = 16384  # the encoder's tile of rows
     yield "every row a run", orc.uniform_bits(5, 40, 5 * t + 3)
     yield "one run over many tiles", np.full(37 * t + 11, 123456789, dtype=np.uint64)
     yield "two runs, boundary mid-tile", np.concatenate([np.full(9 * t + 700, 7, np.uint64),
@@ -152,9 +153,21 @@ def _rle_cases(orc):
     yield "runs of 64-bit values", orc.runs(8, 3, 64, 10 * t + 9)
     for k in (t - 1, t, t + 1, 2 * t - 1, 2 * t + 1):
         yield f"runs, n={k}", orc.runs(9 + k, 2, 8, k)
+    yield "every row a run, 40 encoder tiles", orc.uniform_bits(10, 30, 40 * T + 5)
+    for k in (T - 1, T, T + 1, 3 * T - 1, 3 * T + 1):
+        yield f"short runs, n={k}", orc.runs(11 + k, 1, 8, k)
+    yield "runs ending on encoder tiles", np.repeat(orc.uniform_bits(12, 20, 24), T)
+    yield "long runs, small decoder tiles", orc.runs(13, 7, 20, 300 * T + 77)
 
 
-@pytest.mark.parametrize("case", range(12))
+N_RLE_CASES = 20
+
+
+def test_rle_case_count(orc):
+    assert len(list(_rle_cases(orc))) == N_RLE_CASES
+
+
+@pytest.mark.parametrize("case", range(N_RLE_CASES))
 def test_rle_codec_edge_cases(ms, arena, orc, case):
     name, v = list(_rle_cases(orc))[case]
     c = ms.morph(ms.Column.from_numpy(v, arena), ms.rle_f)
@@ -162,6 +175,31 @@ def test_rle_codec_edge_cases(ms, arena, orc, case):
     assert c.meta() == m, name
     assert np.array_equal(c.raw_bytes(), b), name
     assert np.array_equal(c.to_numpy(), v), name
+
+
+@pytest.mark.parametrize("mean_log2", [0, 5, 9])
+def test_rle_decode_zero_length_runs(ms, arena, orc, mean_log2):
+    """Pairs with length 0 write nothing (rle.h:238-249): bursts of them at
+    the start, inside and at the end of the column, longer than a warp's
+    window and across decoder tiles, decode as the oracle decodes them."""
+    v = orc.runs(14 + mean_log2, mean_log2, 20, 200_003) if mean_log2 else orc.uniform_bits(14, 20, 200_003)
+    b, m = orc.compress(O.RLE, 0, v)
+    pairs = b.view(np.uint64).reshape(-1, 2)
+    rng = np.random.default_rng(mean_log2)
+    at = np.sort(rng.choice(len(pairs), size=min(300, len(pairs)), replace=False))
+    burst = np.array([[7, 0]] * 70, dtype=np.uint64)
+    parts, last = [burst], 0
+    for i, k in enumerate(at):
+        parts.append(pairs[last:k])
+        parts.append(burst[: 1 + (i % 5) * 10])
+        last = k
+    parts += [pairs[last:], burst[:3]]
+    z = np.ascontiguousarray(np.concatenate(parts).astype(np.uint64)).reshape(-1)
+    zm = (m[0], z.nbytes, z.nbytes)
+    want = orc.decompress(O.RLE, 0, z.view(np.uint8), zm)
+    assert np.array_equal(want, v)
+    col = ms.Column.from_bytes(ms.rle_f, z.view(np.uint8), zm, arena)
+    assert np.array_equal(ms.morph(col, ms.uncompr_f).to_numpy(), want)
 
 
 def test_rle_decode_reports_inconsistent_lengths(ms, arena, orc):
