@@ -101,6 +101,7 @@ _sig = {
     "ms_gpu_batch_info": (C.c_int, [_V, _P(_U64), _P(_U64)]),
     "ms_gpu_batch_destroy": (None, [_V]),
     "ms_gpu_get_query_tuning": (C.c_int, [_P(MsTuning)]),
+    "ms_gpu_query3_last_pass_ms": (C.c_int, [_P(C.c_double)]),
     "ms_gpu_get_tuning": (C.c_int, [_P(MsTuning)]),
     "ms_gpu_gen_uniform_bits": (C.c_int, [_U64, C.c_uint, _U64, _V, _V]),
     "ms_gpu_gen_uniform_bits_at": (C.c_int, [_U64, C.c_uint, _U64, _U64, _V, _V]),
@@ -536,6 +537,14 @@ def set_query_tuning(staged: int = 1, warps: int = 16, stages: int = 3, stage_by
     t = MsTuning(staged=staged, warps=warps, stages=stages, stage_bytes=stage_bytes, ctas_per_sm=1,
                  values_per_thread=16)
     _check(_lib.ms_gpu_set_query_tuning(C.byref(t)), "set_query_tuning")
+
+
+def query3_last_pass_ms() -> float:
+    """Device time of the last query3 call's fact-table pass, in ms (-1 before
+    the first call)."""
+    v = C.c_double()
+    _check(_lib.ms_gpu_query3_last_pass_ms(C.byref(v)), "query3_last_pass_ms")
+    return float(v.value)
 
 
 def get_query_tuning() -> dict:

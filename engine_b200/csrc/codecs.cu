@@ -18,6 +18,7 @@
 
 #include "internal.h"
 #include "scan.cuh"
+#include "tma.cuh"
 
 namespace ms {
 namespace {
@@ -400,6 +401,136 @@ __global__ void __launch_bounds__(kRleEncThreads) k_rle_encode(const uint64_t *_
     }
 }
 
+// Staged encoder: the same algorithm, one tile of kRleStThreads *
+// kRleRowsPerThread rows per CTA, with the tile's rows brought into shared
+// memory by asynchronous 16-byte copies (cp.async) that are all in flight at
+// once instead of one register load per step; each lane compares its row
+// with the one before it in shared memory.  Three CTAs per SM, so one CTA's
+// look-back overlaps the others' reads.  Needs a 16-byte aligned input.
+constexpr unsigned kRleStThreads = 512;
+constexpr unsigned kRleStTile = kRleStThreads * kRleRowsPerThread;
+
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+
+__global__ void __launch_bounds__(kRleStThreads) k_rle_encode_staged(const uint64_t *__restrict__ in, uint64_t n,
+                                                                    RleTileState *state, unsigned *ticket,
+                                                                    uint64_t *__restrict__ out,
+                                                                    uint64_t *__restrict__ d_runs, unsigned *err) {
+    constexpr unsigned NW = kRleStThreads / 32, WR = 32 * kRleRowsPerThread;
+    extern __shared__ __align__(128) uint8_t rle_smem[];
+    uint64_t *const v = reinterpret_cast<uint64_t *>(rle_smem);  // the tile's rows
+    __shared__ uint64_t s_tile;
+    __shared__ unsigned s_ball[NW][kRleRowsPerThread];
+    __shared__ unsigned s_wcnt[NW];
+    __shared__ uint64_t s_wlast[NW];
+    __shared__ uint64_t s_excl_runs, s_excl_last;
+    const unsigned lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+    if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
+    __syncthreads();
+    const uint64_t tile = s_tile;
+    const uint64_t ntiles = (n + kRleStTile - 1) / kRleStTile;
+    if (tile >= ntiles) return;
+    const uint64_t r0 = tile * kRleStTile;
+    const unsigned rows = unsigned(minu(kRleStTile, n - r0));
+    {
+        // every 16-byte pair of rows of the tile, consecutive threads on
+        // consecutive pairs; an odd last row of the column is read directly
+        const unsigned pairs = rows / 2;
+        for (unsigned q = threadIdx.x; q < pairs; q += kRleStThreads) cp_async16(v + 2 * q, in + r0 + 2 * q);
+        asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+        if ((rows & 1u) && threadIdx.x == 0) v[rows - 1] = __ldg(in + r0 + rows - 1);
+    }
+    __syncthreads();
+    // heads: warp w covers tile rows [w WR, (w + 1) WR), lane-strided; the
+    // tile's first row is compared with the previous tile's last
+    const unsigned wbase = wid * WR;
+    const uint64_t before = r0 ? __ldg(in + r0 - 1) : 0;
+    unsigned c = 0;
+    uint64_t my_last = 0;  // last head of this warp as row + 1 (0: none)
+#pragma unroll
+    for (unsigned k = 0; k < kRleRowsPerThread; k++) {
+        const unsigned lr = wbase + 32 * k + lane;
+        const bool valid = lr < rows;
+        const uint64_t x = valid ? v[lr] : 0;
+        const uint64_t prev = lr ? v[lr - 1] : before;
+        const unsigned bk = __ballot_sync(0xFFFFFFFFu, valid && (r0 + lr == 0 || x != prev));
+        if (lane == 0) s_ball[wid][k] = bk;
+        c += __popc(bk);
+        if (bk) my_last = r0 + wbase + 32 * k + (31 - __clz(bk)) + 1;
+    }
+    if (lane == 0) {
+        s_wcnt[wid] = c;
+        s_wlast[wid] = my_last;
+    }
+    __syncthreads();
+    if (wid == 0) {
+        // the whole tile: runs and last head; publish, then look back
+        uint64_t agg_runs = lane < NW ? s_wcnt[lane] : 0, agg_last = lane < NW ? s_wlast[lane] : 0;
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) {
+            agg_runs += __shfl_xor_sync(0xFFFFFFFFu, agg_runs, d);
+            agg_last = maxu(agg_last, __shfl_xor_sync(0xFFFFFFFFu, agg_last, d));
+        }
+        RleTileState *me = state + tile;
+        const uint64_t own_last = agg_last ? agg_last - 1 : kRleNone;
+        uint64_t excl_runs = 0, excl_last = kRleNone;
+        if (tile > 0) {
+            if (lane == 0) {
+                me->agg_runs = agg_runs;
+                me->agg_last = own_last;
+                __threadfence();
+                atomicExch(&me->flag, kRleFlagAgg);
+            }
+            __syncwarp();
+            if (!rle_lookback(state, tile, excl_runs, excl_last) && lane == 0) atomicOr(err, kErrTimeout);
+        }
+        if (lane == 0) {
+            me->inc_runs = excl_runs + agg_runs;
+            me->inc_last = own_last != kRleNone ? own_last : excl_last;
+            __threadfence();
+            atomicExch(&me->flag, kRleFlagInc);
+            s_excl_runs = excl_runs;
+            s_excl_last = excl_last;
+            if (tile == ntiles - 1) {
+                // the final run ends at row n
+                const uint64_t total = excl_runs + agg_runs;
+                const uint64_t last = own_last != kRleNone ? own_last : excl_last;
+                *d_runs = total;
+                if (total) out[2 * (total - 1) + 1] = n - last;
+            }
+        }
+    }
+    __syncthreads();
+    // pairs: every head writes its run's value and the length of the run
+    // before it; consecutive lanes write consecutive pairs
+    unsigned wpre = 0;
+    uint64_t wlast = 0;
+    for (unsigned w = 0; w < wid; w++) {
+        wpre += s_wcnt[w];
+        wlast = maxu(wlast, s_wlast[w]);
+    }
+    uint64_t k_run = s_excl_runs + wpre;                   // run index of the warp's next head
+    uint64_t prev_head = wlast ? wlast - 1 : s_excl_last;  // row of the head before it
+    const unsigned below = (1u << lane) - 1u;
+#pragma unroll 4
+    for (unsigned k = 0; k < kRleRowsPerThread; k++) {
+        const unsigned bk = s_ball[wid][k];
+        if (!bk) continue;
+        const unsigned lr = wbase + 32 * k + lane;
+        if ((bk >> lane) & 1u) {
+            const uint64_t idx = k_run + __popc(bk & below);
+            const unsigned lower = bk & below;
+            const uint64_t ph = lower ? r0 + wbase + 32 * k + (31 - __clz(lower)) : prev_head;
+            out[2 * idx] = v[lr];
+            if (idx) out[2 * (idx - 1) + 1] = r0 + lr - ph;
+        }
+        k_run += __popc(bk);
+        prev_head = r0 + wbase + 32 * k + (31 - __clz(bk));
+    }
+}
+
 constexpr unsigned kRleThreads = 256;
 constexpr unsigned kRleRunsPerThread = 8;
 constexpr unsigned kRleTile = kRleThreads * kRleRunsPerThread;  // most runs per decoder tile
@@ -590,7 +721,8 @@ __global__ void __launch_bounds__(kRleThreads) k_rle_expand(const uint64_t *__re
 // host drivers
 // ---------------------------------------------------------------------------
 static int encode_rle(const uint64_t *d_in, uint64_t n, ms_col *out, ms_arena *a, cudaStream_t st) {
-    const uint64_t tiles = (n + kRleEncTile - 1) / kRleEncTile;
+    // tile states for the smaller of the two encoders' tiles
+    const uint64_t tiles = (n + minu(kRleEncTile, kRleStTile) - 1) / minu(kRleEncTile, kRleStTile);
     uint8_t *data = arena_take_t<uint8_t>(a, 16 * n + 64);
     RleTileState *state = arena_take_t<RleTileState>(a, tiles + 1);
     unsigned *ticket = arena_take_t<unsigned>(a, 2);
@@ -600,8 +732,17 @@ static int encode_rle(const uint64_t *d_in, uint64_t n, ms_col *out, ms_arena *a
     if (n) {
         MS_CUDA_TRY(cudaMemsetAsync(state, 0, sizeof(RleTileState) * tiles, st));
         MS_CUDA_TRY(cudaMemsetAsync(ticket, 0, sizeof(unsigned), st));
-        k_rle_encode<<<unsigned(tiles), kRleEncThreads, 0, st>>>(d_in, n, state, ticket, (uint64_t *)data, d_runs,
-                                                                 a->d_err);
+        if ((reinterpret_cast<uintptr_t>(d_in) & 15u) == 0) {
+            // rows staged in shared memory (16-byte aligned input)
+            constexpr size_t smem = size_t(kRleStTile) * 8;
+            MS_CUDA_TRY(cudaFuncSetAttribute(k_rle_encode_staged, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             int(smem)));
+            k_rle_encode_staged<<<unsigned((n + kRleStTile - 1) / kRleStTile), kRleStThreads, smem, st>>>(
+                d_in, n, state, ticket, (uint64_t *)data, d_runs, a->d_err);
+        } else {
+            k_rle_encode<<<unsigned((n + kRleEncTile - 1) / kRleEncTile), kRleEncThreads, 0, st>>>(
+                d_in, n, state, ticket, (uint64_t *)data, d_runs, a->d_err);
+        }
         MS_CUDA_TRY(cudaGetLastError());
         MS_CUDA_TRY(cudaMemcpyAsync(&runs, d_runs, 8, cudaMemcpyDeviceToHost, st));
         int rc = read_err(a, st);  // synchronises the stream

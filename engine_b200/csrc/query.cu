@@ -182,14 +182,43 @@ __host__ __device__ inline uint64_t q3_meta_bytes(unsigned S) {
     return (uint64_t(16) * S + sizeof(QStage) * S + 5ull * kQCols * S * kQTile + 127) / 128 * 128;
 }
 
-// kSB: the build side's bitmap (nwords words) is copied into shared memory
-// after the group table, so the probes cost a shared-memory load instead of
-// an L2 round trip.
-template <int W, bool kSB>
+// Where the probes read the build side's bitmap (nwords words):
+enum : int {
+    kBmGlobal = 0,   // global memory (an L2 round trip per probe)
+    kBmShared = 1,   // the whole bitmap in this CTA's shared memory
+    kBmCluster = 2,  // split over the two CTAs of a cluster: words [0, half) in
+                     // rank 0, [half, nwords) in rank 1, read through
+                     // distributed shared memory (ld.shared::cluster)
+};
+
+__device__ __forceinline__ unsigned cluster_rank() {
+    unsigned r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+
+// every thread of both CTAs of the cluster; shared-memory writes before it
+// are visible to the other CTA after it
+__device__ __forceinline__ void cluster_sync() {
+    asm volatile("barrier.cluster.arrive.release;\n\tbarrier.cluster.wait.acquire;" ::: "memory");
+}
+
+__device__ __forceinline__ uint32_t dsmem_ld32(const uint32_t *local_base, uint32_t idx, unsigned rank) {
+    uint32_t a, v;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(a) : "r"(smem_u32(local_base + idx)), "r"(rank));
+    asm volatile("ld.shared::cluster.u32 %0, [%1];" : "=r"(v) : "r"(a) : "memory");
+    return v;
+}
+
+// kBM: where the bitmap lives (kBmGlobal / kBmShared / kBmCluster); in
+// shared memory it follows the group table, so a probe costs a shared-memory
+// load (local or in the partner CTA) instead of an L2 round trip.
+template <int W, int kBM>
 __global__ void __launch_bounds__(32 * (W + 1), 1)
     k_query3_tma(ColView fk, ColView gkey, ColView meas, StreamCol c0, StreamCol c1, StreamCol c2, StreamCol c3,
                  Pred pred, const uint32_t *__restrict__ bits, uint64_t nwords, uint64_t lo, uint64_t span, QCfg cfg,
                  GTable gt, uint32_t *__restrict__ blk_hits, unsigned *err) {
+    constexpr bool kSB = kBM != kBmGlobal;
     extern __shared__ __align__(128) uint8_t smem[];
     const unsigned S = cfg.stages, SB = cfg.stage_bytes;
     uint64_t *full = reinterpret_cast<uint64_t *>(smem);
@@ -210,8 +239,13 @@ __global__ void __launch_bounds__(32 * (W + 1), 1)
         s_first[i] = ~0ull;
         s_sum[i] = 0;
     }
-    if (kSB)
+    const uint32_t half = uint32_t((nwords + 1) / 2);  // words per CTA in a cluster
+    if (kBM == kBmShared)
         for (uint64_t i = threadIdx.x; i < nwords; i += blockDim.x) s_bits[i] = __ldg(bits + i);
+    if (kBM == kBmCluster) {
+        const uint64_t w0 = uint64_t(cluster_rank()) * half;
+        for (uint64_t i = threadIdx.x; i < half; i += blockDim.x) s_bits[i] = w0 + i < nwords ? __ldg(bits + w0 + i) : 0u;
+    }
     if (threadIdx.x == 0) {
         for (unsigned st = 0; st < S; st++) {
             mbar_init(full + st, 1);
@@ -220,6 +254,7 @@ __global__ void __launch_bounds__(32 * (W + 1), 1)
         mbar_fence_init();
     }
     __syncthreads();
+    if (kBM == kBmCluster) cluster_sync();  // both halves of the bitmap are in place
 
     const uint64_t nbs = minu(minu(c0.nb, c1.nb), minu(c2.nb, c3.nb));
     const uint64_t b_lo = nbs * blockIdx.x / gridDim.x, b_hi = nbs * (blockIdx.x + 1) / gridDim.x;
@@ -351,7 +386,13 @@ __global__ void __launch_bounds__(32 * (W + 1), 1)
                             const uint64_t v = vbp_extract(kb, kbw, l, 16u * q + kk[i]) + kref;
                             const uint64_t d = v - lo;
                             inr[i] = had[i] && v >= lo && d < span;
-                            word[i] = inr[i] ? (kSB ? pbits[d >> 5] : __ldg(pbits + (d >> 5))) : 0u;
+                            if (kBM == kBmCluster) {
+                                const uint32_t wi = uint32_t(d >> 5);
+                                const unsigned own = wi >= half;
+                                word[i] = inr[i] ? dsmem_ld32(s_bits, wi - own * half, own) : 0u;
+                            } else {
+                                word[i] = inr[i] ? (kSB ? pbits[d >> 5] : __ldg(pbits + (d >> 5))) : 0u;
+                            }
                             bit[i] = unsigned(d & 31u);
                         }
 #pragma unroll
@@ -420,6 +461,7 @@ __global__ void __launch_bounds__(32 * (W + 1), 1)
     if (!ok) atomicOr(err, kErrTimeout);
     if (bad) atomicOr(err, kErrCorrupt);
     if (!fit) atomicOr(err, kErrCapacity);
+    if (kBM == kBmCluster) cluster_sync();  // the partner may still read this CTA's half
 }
 
 // bitmap of the build side's keys (dense range)
@@ -515,33 +557,82 @@ constexpr size_t kQSmemMax = 232448;  // 227 KiB of dynamic shared memory per CT
 
 // launch configuration of the staged kernel (consumer warps 8/16/24)
 ms_tuning g_q3 = {1, 16, 3, 57344, 1, 16};
+// device time of the last call's fact-table pass
+cudaEvent_t g_q3_ev[2] = {nullptr, nullptr};
+double g_q3_pass_ms = -1;
+
+template <int W, int kBM>
+int launch_q3_kern(size_t shm, QCfg cfg, const ColView &kv, const ColView &gv, const ColView &mv,
+                   const StreamCol &s0, const StreamCol &s1, const StreamCol &s2, const StreamCol &s3, const Pred &pred,
+                   const uint32_t *bits, uint64_t nwords, uint64_t lo, uint64_t span, const GTable &gt, uint32_t *hits,
+                   unsigned *d_err, cudaStream_t st) {
+    auto kern = k_query3_tma<W, kBM>;
+    MS_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
+    if (kBM != kBmCluster) {
+        kern<<<unsigned(sm_count()), 32 * (W + 1), shm, st>>>(kv, gv, mv, s0, s1, s2, s3, pred, bits, nwords, lo, span,
+                                                              cfg, gt, hits, d_err);
+        MS_CUDA_TRY(cudaGetLastError());
+        return MS_OK;
+    }
+    // clusters of two CTAs (one per SM), as many as fit at once
+    cudaLaunchConfig_t lc = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = 2;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    lc.blockDim = dim3(32 * (W + 1));
+    lc.dynamicSmemBytes = shm;
+    lc.stream = st;
+    lc.attrs = at;
+    lc.numAttrs = 1;
+    lc.gridDim = dim3(unsigned(sm_count() / 2 * 2));
+    int ncl = 0;
+    MS_CUDA_TRY(cudaOccupancyMaxActiveClusters(&ncl, kern, &lc));
+    lc.gridDim = dim3(unsigned(2 * (ncl > 0 ? ncl : 1)));
+    MS_CUDA_TRY(cudaLaunchKernelEx(&lc, kern, kv, gv, mv, s0, s1, s2, s3, pred, bits, nwords, lo, span, cfg, gt, hits,
+                                   d_err));
+    return MS_OK;
+}
 
 template <int W>
 int launch_q3_tma_w(const ColView &kv, const ColView &gv, const ColView &mv, const StreamCol &s0, const StreamCol &s1,
                     const StreamCol &s2, const StreamCol &s3, const Pred &pred, const uint32_t *bits, uint64_t nwords,
                     uint64_t lo, uint64_t span, const GTable &gt, uint32_t *hits, unsigned *d_err, cudaStream_t st) {
-    const QCfg cfg{g_q3.stages, g_q3.stage_bytes};
-    const size_t table = 3ull * 8 * kQSlots, bitmap = 4 * nwords;
-    size_t shm = q3_meta_bytes(cfg.stages) + size_t(cfg.stages) * cfg.stage_bytes + table;
-    // The bitmap goes to shared memory when it fits beside the ring.  (Shrinking
-    // the ring to make room for a large bitmap was measured slower: a 2^20-key
-    // build side with a 2 x 25 KiB ring lost more to the shallower pipeline
-    // than the probes gained.)
-    const bool sb = g_q3.staged == 1 && shm + bitmap <= kQSmemMax;
-    shm = q3_meta_bytes(cfg.stages) + size_t(cfg.stages) * cfg.stage_bytes + table + (sb ? bitmap : 0);
-    if (sb) {
-        auto kern = k_query3_tma<W, true>;
-        MS_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
-        kern<<<unsigned(sm_count()), 32 * (W + 1), shm, st>>>(kv, gv, mv, s0, s1, s2, s3, pred, bits, nwords, lo,
-                                                              span, cfg, gt, hits, d_err);
-    } else {
-        auto kern = k_query3_tma<W, false>;
-        MS_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
-        kern<<<unsigned(sm_count()), 32 * (W + 1), shm, st>>>(kv, gv, mv, s0, s1, s2, s3, pred, bits, nwords, lo,
-                                                              span, cfg, gt, hits, d_err);
+    QCfg cfg{g_q3.stages, g_q3.stage_bytes};
+    const size_t table = 3ull * 8 * kQSlots, bitmap = 4 * nwords, half = 4 * ((nwords + 1) / 2);
+    const size_t meta = q3_meta_bytes(cfg.stages);
+    const size_t ring = size_t(cfg.stages) * cfg.stage_bytes;
+    // staged 1: the bitmap in shared memory -- whole beside the configured
+    // ring when it fits, else split over a 2-CTA cluster with the ring's
+    // stages shrunk to make room (down to 24 KiB), else in global memory.
+    // staged 3: always split over a cluster.  (Shrinking the ring to keep a
+    // large bitmap whole in one CTA was measured slower: a 2^20-key build
+    // side with a 2 x 25 KiB ring lost more to the shallower pipeline than
+    // the probes gained.)
+    const auto fit_stage = [&](size_t words_bytes) -> unsigned {
+        if (meta + table + words_bytes >= kQSmemMax) return 0;
+        const size_t room = kQSmemMax - meta - table - words_bytes;
+        const size_t sb = minu(cfg.stage_bytes, room / cfg.stages / 128 * 128);
+        return sb >= 24576 ? unsigned(sb) : 0;
+    };
+    int mode = kBmGlobal;
+    if (g_q3.staged == 1 && meta + ring + table + bitmap <= kQSmemMax) mode = kBmShared;
+    else if ((g_q3.staged == 1 || g_q3.staged == 3) && fit_stage(half)) mode = kBmCluster;
+    if (mode == kBmCluster) cfg.stage_bytes = fit_stage(half);
+    const size_t shm = meta + size_t(cfg.stages) * cfg.stage_bytes + table +
+                       (mode == kBmShared ? bitmap : mode == kBmCluster ? half : 0);
+    switch (mode) {
+    case kBmShared:
+        return launch_q3_kern<W, kBmShared>(shm, cfg, kv, gv, mv, s0, s1, s2, s3, pred, bits, nwords, lo, span, gt,
+                                            hits, d_err, st);
+    case kBmCluster:
+        return launch_q3_kern<W, kBmCluster>(shm, cfg, kv, gv, mv, s0, s1, s2, s3, pred, bits, nwords, lo, span, gt,
+                                             hits, d_err, st);
+    default:
+        return launch_q3_kern<W, kBmGlobal>(shm, cfg, kv, gv, mv, s0, s1, s2, s3, pred, bits, nwords, lo, span, gt,
+                                            hits, d_err, st);
     }
-    MS_CUDA_TRY(cudaGetLastError());
-    return MS_OK;
 }
 
 int launch_q3_tma(const ColView &kv, const ColView &gv, const ColView &mv, const StreamCol &s0, const StreamCol &s1,
@@ -561,13 +652,15 @@ using namespace ms;
 
 // Launch configuration of the fused query's staged kernel: staged (0 = the
 // direct kernel only, 1 = staged with the build-side bitmap in shared memory
-// when it fits, 2 = staged with the bitmap in global memory), warps
+// -- whole when it fits beside the ring, else split over a 2-CTA cluster --
+// 2 = staged with the bitmap in global memory, 3 = staged with the bitmap
+// always split over a 2-CTA cluster), warps
 // (consumer warps: 8, 16 or 24), stages and
 // stage_bytes (shared-memory ring; stages x stage_bytes + 48 KiB group table
 // must fit 227 KiB).  The other fields are ignored.
 extern "C" int ms_gpu_set_query_tuning(const ms_tuning *t) {
     if (!t) return ms_fail(MS_ERR_INVALID, "set_query_tuning: null");
-    if (t->staged > 2) return ms_fail(MS_ERR_INVALID, "set_query_tuning: staged must be 0, 1 or 2");
+    if (t->staged > 3) return ms_fail(MS_ERR_INVALID, "set_query_tuning: staged must be 0, 1, 2 or 3");
     if (t->warps != 8 && t->warps != 16 && t->warps != 24)
         return ms_fail(MS_ERR_INVALID, "set_query_tuning: warps must be 8, 16 or 24");
     if (t->stages < 2 || t->stages > 16 || t->stage_bytes % 128 || t->stage_bytes < 16384)
@@ -575,6 +668,12 @@ extern "C" int ms_gpu_set_query_tuning(const ms_tuning *t) {
     if (q3_meta_bytes(t->stages) + uint64_t(t->stages) * t->stage_bytes + 3ull * 8 * kQSlots > 232448)
         return ms_fail(MS_ERR_INVALID, "set_query_tuning: shared memory above 227 KiB");
     g_q3 = *t;
+    return MS_OK;
+}
+
+extern "C" int ms_gpu_query3_last_pass_ms(double *ms) {
+    if (!ms) return ms_fail(MS_ERR_INVALID, "query3_last_pass_ms: null");
+    *ms = g_q3_pass_ms;
     return MS_OK;
 }
 
@@ -655,6 +754,11 @@ extern "C" int ms_gpu_query3(const ms_col *filter, int cmp, uint64_t c, const ms
         MS_CUDA_TRY(cudaMemsetAsync(gt.sums, 0, 8 * slots, st));
         MS_CUDA_TRY(cudaMemsetAsync(cnt, 0, 8, st));
         MS_CUDA_TRY(cudaMemsetAsync(tot, 0, 8, st));
+        if (!g_q3_ev[0]) {
+            MS_CUDA_TRY(cudaEventCreate(&g_q3_ev[0]));
+            MS_CUDA_TRY(cudaEventCreate(&g_q3_ev[1]));
+        }
+        MS_CUDA_TRY(cudaEventRecord(g_q3_ev[0], st));
         if (nbt) {
             uint64_t nbs = 0;  // blocks through the staged kernel
             if (g_q3.staged && plain(fv) && random_access(kv) && random_access(gv) && random_access(mv)) {
@@ -671,6 +775,7 @@ extern "C" int ms_gpu_query3(const ms_col *filter, int cmp, uint64_t c, const ms
                 k_query3<<<g2, 256, 0, st>>>(fv, kv, gv, mv, cmp, c, bits, lo, span, gt, hits, nbs, a->d_err);
                 MS_CUDA_TRY(cudaGetLastError());
             }
+            MS_CUDA_TRY(cudaEventRecord(g_q3_ev[1], st));
             MS_CUDA_TRY((scan_exclusive<uint32_t, 1>(hits, nbt, boff, tot, scr, st)));
             k_q3_extents<<<unsigned(minu(slots / 8, 4096)), 256, 0, st>>>(
                 gt, fv, kv, cmp, c, bits, lo, span, boff, cnt, out, a->d_err);
@@ -695,6 +800,8 @@ extern "C" int ms_gpu_query3(const ms_col *filter, int cmp, uint64_t c, const ms
         }
         rc = read_err(a, st);
         if (rc) return rc;
+        float pass_ms = 0;
+        if (nbt && cudaEventElapsedTime(&pass_ms, g_q3_ev[0], g_q3_ev[1]) == cudaSuccess) g_q3_pass_ms = pass_ms;
         ng = hc[0];
         np = hc[1];
         if (ng > first) {

@@ -285,12 +285,20 @@ int ms_gpu_query3(const ms_col *filter, int cmp, uint64_t c, const ms_col *fk, c
                   ms_arena *arena, void *stream);
 /* Launch configuration of ms_gpu_query3's staged kernel (no counterpart in
  * the reference): staged (0 = direct kernel only, 1 = staged with the
- * build side's bitmap in shared memory when it fits, 2 = staged with the
- * bitmap in global memory), warps (consumer warps 8,
- * 16 or 24), stages, stage_bytes; other fields ignored.  Rejects a ring that
- * does not fit shared memory with the 48 KiB group table. */
+ * build side's bitmap in shared memory -- whole when it fits beside the
+ * ring, else split over a 2-CTA cluster with the ring's stages shrunk to
+ * make room, else in global memory -- 2 = staged with the bitmap in global
+ * memory, 3 = staged with the bitmap always split over a 2-CTA cluster),
+ * warps (consumer warps 8, 16 or 24), stages, stage_bytes; other fields
+ * ignored.  Rejects a ring that does not fit shared memory with the 48 KiB
+ * group table. */
 int ms_gpu_set_query_tuning(const ms_tuning *t);
 int ms_gpu_get_query_tuning(ms_tuning *t);
+/* Device time (CUDA events around the fact-table pass: the staged kernel and
+ * the direct kernel for the rest) of the last successful ms_gpu_query3 call
+ * in this process, in ms; -1 before the first.  For measurement only (no
+ * counterpart in the reference). */
+int ms_gpu_query3_last_pass_ms(double *ms);
 
 /* ---- batched persistent execution (no counterpart as one call in the
  * reference: for every column i it runs the chain morph<uncompr_f> ->

@@ -130,7 +130,10 @@ def test_query3_rejects_bad_input(ms, arena, orc):
 @pytest.mark.parametrize("cfg", [dict(staged=0), dict(staged=2, warps=16, stages=3, stage_bytes=57344),
                                  dict(warps=8, stages=2, stage_bytes=16384),
                                  dict(warps=16, stages=4, stage_bytes=40960),
-                                 dict(warps=24, stages=3, stage_bytes=57344)])
+                                 dict(warps=24, stages=3, stage_bytes=57344),
+                                 dict(staged=3, warps=16, stages=3, stage_bytes=57344),
+                                 dict(staged=3, warps=8, stages=2, stage_bytes=32768),
+                                 dict(staged=3, warps=24, stages=4, stage_bytes=40960)])
 def test_query3_launch_configs(ms, arena, orc, cfg):
     """Every staged-kernel configuration (and the direct kernel alone) gives
     the oracle's groups; ragged length so the tail kernel runs too."""
@@ -147,6 +150,30 @@ def test_query3_launch_configs(ms, arena, orc, cfg):
         ms.set_query_tuning(**old)
     sf = orc.scalar_from(O.DYNAMIC_VBP, 0, cols[0].meta())
     ek, ee, es, enp = _expect(orc, O.CMP_LT, 1000, filt, fk, gkey, meas, lk, sf)
+    assert (npos, len(keys)) == (enp, len(ek))
+    assert np.array_equal(keys, ek) and np.array_equal(ext, ee) and np.array_equal(sums, es)
+
+
+@pytest.mark.parametrize("staged", [1, 2, 3])
+def test_query3_wide_build_side(ms, arena, orc, staged):
+    """A build side over 2^20 keys: its 128 KB bitmap does not fit one CTA
+    beside the ring, so staged=1 splits it over a 2-CTA cluster (read through
+    distributed shared memory), as staged=3 always does; staged=2 reads it
+    from global memory.  All equal the oracle, and the pass time is recorded."""
+    n = 1_000_003
+    filt, fk, gkey, meas, lk = _data(orc, n, seed=31, key_bits=20, keep=1)
+    codes = (O.DYNAMIC_VBP, O.DYNAMIC_VBP, O.FOR_DVBP, O.DYNAMIC_VBP)
+    cols = [_col(ms, arena, orc, v, code) for v, code in zip((filt, fk, gkey, meas), codes)]
+    lcol = _col(ms, arena, orc, lk, O.DELTA_DVBP)
+    old = ms.get_query_tuning()
+    try:
+        ms.set_query_tuning(staged=staged, warps=16, stages=3, stage_bytes=57344)
+        keys, ext, sums, npos = ms.query3(cols[0], O.CMP_LT, 400, cols[1], lcol, cols[2], cols[3])
+    finally:
+        ms.set_query_tuning(**old)
+    assert ms.query3_last_pass_ms() > 0
+    sf = orc.scalar_from(O.DYNAMIC_VBP, 0, cols[0].meta())
+    ek, ee, es, enp = _expect(orc, O.CMP_LT, 400, filt, fk, gkey, meas, lk, sf)
     assert (npos, len(keys)) == (enp, len(ek))
     assert np.array_equal(keys, ek) and np.array_equal(ext, ee) and np.array_equal(sums, es)
 
