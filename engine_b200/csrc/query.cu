@@ -603,13 +603,15 @@ int launch_q3_tma_w(const ColView &kv, const ColView &gv, const ColView &mv, con
     const size_t table = 3ull * 8 * kQSlots, bitmap = 4 * nwords, half = 4 * ((nwords + 1) / 2);
     const size_t meta = q3_meta_bytes(cfg.stages);
     const size_t ring = size_t(cfg.stages) * cfg.stage_bytes;
-    // staged 1: the bitmap in shared memory -- whole beside the configured
-    // ring when it fits, else split over a 2-CTA cluster with the ring's
-    // stages shrunk to make room (down to 24 KiB), else in global memory.
-    // staged 3: always split over a cluster.  (Shrinking the ring to keep a
-    // large bitmap whole in one CTA was measured slower: a 2^20-key build
-    // side with a 2 x 25 KiB ring lost more to the shallower pipeline than
-    // the probes gained.)
+    // staged 1: the bitmap in shared memory beside the configured ring when
+    // it fits, else in global memory.  staged 3: split over a 2-CTA cluster,
+    // the ring's stages shrunk to make room (down to 24 KiB).  Both ways of
+    // making room for a large bitmap were measured slower than reading it
+    // from global memory: for a 2^20-key build side a 2 x 25 KiB ring with
+    // the whole bitmap lost more to the shallower pipeline than the probes
+    // gained, and the cluster split (3 x 38 KiB ring, half the bitmap per
+    // CTA) took 242 us at 2^26 fact rows against 198 us, its distributed
+    // shared-memory probes stalling longer than the L2 ones.
     const auto fit_stage = [&](size_t words_bytes) -> unsigned {
         if (meta + table + words_bytes >= kQSmemMax) return 0;
         const size_t room = kQSmemMax - meta - table - words_bytes;
@@ -618,7 +620,7 @@ int launch_q3_tma_w(const ColView &kv, const ColView &gv, const ColView &mv, con
     };
     int mode = kBmGlobal;
     if (g_q3.staged == 1 && meta + ring + table + bitmap <= kQSmemMax) mode = kBmShared;
-    else if ((g_q3.staged == 1 || g_q3.staged == 3) && fit_stage(half)) mode = kBmCluster;
+    else if (g_q3.staged == 3 && fit_stage(half)) mode = kBmCluster;
     if (mode == kBmCluster) cfg.stage_bytes = fit_stage(half);
     const size_t shm = meta + size_t(cfg.stages) * cfg.stage_bytes + table +
                        (mode == kBmShared ? bitmap : mode == kBmCluster ? half : 0);
@@ -652,9 +654,8 @@ using namespace ms;
 
 // Launch configuration of the fused query's staged kernel: staged (0 = the
 // direct kernel only, 1 = staged with the build-side bitmap in shared memory
-// -- whole when it fits beside the ring, else split over a 2-CTA cluster --
-// 2 = staged with the bitmap in global memory, 3 = staged with the bitmap
-// always split over a 2-CTA cluster), warps
+// when it fits beside the ring, 2 = staged with the bitmap in global memory,
+// 3 = staged with the bitmap split over a 2-CTA cluster), warps
 // (consumer warps: 8, 16 or 24), stages and
 // stage_bytes (shared-memory ring; stages x stage_bytes + 48 KiB group table
 // must fit 227 KiB).  The other fields are ignored.

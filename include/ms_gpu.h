@@ -285,10 +285,10 @@ int ms_gpu_query3(const ms_col *filter, int cmp, uint64_t c, const ms_col *fk, c
                   ms_arena *arena, void *stream);
 /* Launch configuration of ms_gpu_query3's staged kernel (no counterpart in
  * the reference): staged (0 = direct kernel only, 1 = staged with the
- * build side's bitmap in shared memory -- whole when it fits beside the
- * ring, else split over a 2-CTA cluster with the ring's stages shrunk to
- * make room, else in global memory -- 2 = staged with the bitmap in global
- * memory, 3 = staged with the bitmap always split over a 2-CTA cluster),
+ * build side's bitmap in shared memory when it fits beside the ring, else in
+ * global memory, 2 = staged with the bitmap in global memory, 3 = staged
+ * with the bitmap split over a 2-CTA cluster -- half per CTA, read through
+ * distributed shared memory -- with the ring's stages shrunk to make room),
  * warps (consumer warps 8, 16 or 24), stages, stage_bytes; other fields
  * ignored.  Rejects a ring that does not fit shared memory with the 48 KiB
  * group table. */

@@ -157,9 +157,9 @@ def test_query3_launch_configs(ms, arena, orc, cfg):
 @pytest.mark.parametrize("staged", [1, 2, 3])
 def test_query3_wide_build_side(ms, arena, orc, staged):
     """A build side over 2^20 keys: its 128 KB bitmap does not fit one CTA
-    beside the ring, so staged=1 splits it over a 2-CTA cluster (read through
-    distributed shared memory), as staged=3 always does; staged=2 reads it
-    from global memory.  All equal the oracle, and the pass time is recorded."""
+    beside the ring, so staged=1 and 2 read it from global memory and
+    staged=3 splits it over a 2-CTA cluster (read through distributed shared
+    memory).  All equal the oracle, and the pass time is recorded."""
     n = 1_000_003
     filt, fk, gkey, meas, lk = _data(orc, n, seed=31, key_bits=20, keep=1)
     codes = (O.DYNAMIC_VBP, O.DYNAMIC_VBP, O.FOR_DVBP, O.DYNAMIC_VBP)
