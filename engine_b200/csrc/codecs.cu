@@ -715,6 +715,170 @@ __global__ void __launch_bounds__(kRleThreads) k_rle_expand(const uint64_t *__re
     if (blockIdx.x == 0 && threadIdx.x == 0 && *total_rows != n) atomicOr(err, kErrCorrupt);
 }
 
+// One-pass decoder for short runs (mean length <= kRleLbMaxMean): a CTA takes
+// the next tile of kRleLbTile runs from a ticket counter, stages its pairs in
+// shared memory (cp.async), scans the lengths, compacts the non-empty runs to
+// (value, start within the tile), publishes the tile's row count and finds the
+// rows before it by the same decoupled look-back as the encoder (warp 0),
+// then writes the tile's rows in windows of kRleLbWin rows through per-32-row
+// bitmaps of run starts.  Each pair is read once (the two-pass decoder reads
+// every pair twice, which for runs of one row is 32 B read per 8 B written).
+// Shared-memory pairs sit at slot i + i / 8, so that the threads' runs
+// (eight consecutive per thread) fall in different banks.  Writes stop at row
+// n whatever the lengths say; lengths that do not add up to n are reported by
+// the last tile (kErrCorrupt).  Needs 16-byte aligned pairs.
+constexpr unsigned kRleLbThreads = 512, kRleLbRpt = 8;
+constexpr unsigned kRleLbTile = kRleLbThreads * kRleLbRpt;  // runs per tile
+constexpr unsigned kRleLbWin = 8192;                        // rows per write window
+constexpr uint64_t kRleLbMaxMean = 4;
+__host__ __device__ constexpr unsigned rle_lb_slot(unsigned i) { return i + (i >> 3); }
+
+__global__ void __launch_bounds__(kRleLbThreads, 2) k_rle_expand_lb(const uint64_t *__restrict__ pairs,
+                                                                   uint64_t runs, uint64_t n, RleTileState *state,
+                                                                   unsigned *ticket, uint64_t *__restrict__ out,
+                                                                   unsigned *err) {
+    constexpr unsigned NW = kRleLbThreads / 32, NWD = kRleLbWin / 32;
+    extern __shared__ __align__(128) uint8_t rle_smem[];
+    // the tile's pairs, then (value, start within the tile) of its non-empty runs
+    ulonglong2 *const s_p = reinterpret_cast<ulonglong2 *>(rle_smem);
+    __shared__ unsigned s_bits[NWD];
+    __shared__ uint64_t s_wsum[NW];
+    __shared__ unsigned s_wcnt[NW];
+    __shared__ uint64_t s_tile, s_base;
+    const unsigned lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+    const unsigned incl = (2u << lane) - 1u;  // lanes 0..lane
+    if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
+    __syncthreads();
+    const uint64_t tile = s_tile;
+    const uint64_t ntiles = (runs + kRleLbTile - 1) / kRleLbTile;
+    if (tile >= ntiles) return;
+    const uint64_t rb = tile * kRleLbTile;
+    const unsigned nr = unsigned(minu(kRleLbTile, runs - rb));
+    for (unsigned q = threadIdx.x; q < nr; q += kRleLbThreads) cp_async16(s_p + rle_lb_slot(q), pairs + 2 * (rb + q));
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+    __syncthreads();
+    // this thread's kRleLbRpt consecutive runs: scans of lengths and of non-empty runs
+    const unsigned j0 = threadIdx.x * kRleLbRpt;
+    uint64_t len[kRleLbRpt], val[kRleLbRpt], sum = 0;
+    unsigned cnt = 0;
+#pragma unroll
+    for (unsigned k = 0; k < kRleLbRpt; k++) {
+        const ulonglong2 pr = j0 + k < nr ? s_p[rle_lb_slot(j0 + k)] : make_ulonglong2(0, 0);
+        val[k] = pr.x;
+        len[k] = pr.y;
+        sum += len[k];
+        cnt += len[k] != 0;
+    }
+    uint64_t isum = sum;
+    unsigned icnt = cnt;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint64_t o = __shfl_up_sync(0xFFFFFFFFu, isum, d);
+        const unsigned co = __shfl_up_sync(0xFFFFFFFFu, icnt, d);
+        if (int(lane) >= d) {
+            isum += o;
+            icnt += co;
+        }
+    }
+    if (lane == 31) {
+        s_wsum[wid] = isum;
+        s_wcnt[wid] = icnt;
+    }
+    __syncthreads();  // every thread has its pairs in registers: s_p may be overwritten
+    uint64_t ws = lane < NW ? s_wsum[lane] : 0;
+    unsigned wc = lane < NW ? s_wcnt[lane] : 0;
+#pragma unroll
+    for (int d = 1; d < int(NW); d <<= 1) {
+        const uint64_t o = __shfl_up_sync(0xFFFFFFFFu, ws, d);
+        const unsigned co = __shfl_up_sync(0xFFFFFFFFu, wc, d);
+        if (int(lane) >= d) {
+            ws += o;
+            wc += co;
+        }
+    }
+    const uint64_t agg = __shfl_sync(0xFFFFFFFFu, ws, NW - 1);  // the tile's rows
+    const unsigned kept = __shfl_sync(0xFFFFFFFFu, wc, NW - 1);
+    const uint64_t st0 = (wid ? __shfl_sync(0xFFFFFFFFu, ws, wid - 1) : 0) + isum - sum;  // my first run's start
+    {
+        unsigned pos = (wid ? __shfl_sync(0xFFFFFFFFu, wc, wid - 1) : 0) + icnt - cnt;
+        uint64_t run = st0;
+#pragma unroll
+        for (unsigned k = 0; k < kRleLbRpt; k++) {
+            if (len[k]) s_p[rle_lb_slot(pos++)] = make_ulonglong2(val[k], run);
+            run += len[k];
+        }
+    }
+    // publish the tile's rows, then the rows before it
+    RleTileState *me = state + tile;
+    if (threadIdx.x == 0 && tile > 0) {
+        me->agg_runs = agg;
+        me->agg_last = kRleNone;
+        __threadfence();
+        atomicExch(&me->flag, kRleFlagAgg);
+    }
+    if (wid == 0) {
+        uint64_t excl = 0, unused = kRleNone;
+        if (tile > 0 && !rle_lookback(state, tile, excl, unused) && lane == 0) atomicOr(err, kErrTimeout);
+        if (lane == 0) {
+            me->inc_runs = excl + agg;
+            me->inc_last = kRleNone;
+            __threadfence();
+            atomicExch(&me->flag, kRleFlagInc);
+            s_base = excl;
+            if (tile == ntiles - 1 && excl + agg != n) atomicOr(err, kErrCorrupt);
+        }
+    }
+    __syncthreads();
+    const uint64_t base = s_base;
+    if (base >= n) return;
+    const uint64_t rows = minu(agg, n - base);  // never past row n
+    for (uint64_t w0 = 0; w0 < rows; w0 += kRleLbWin) {
+        for (unsigned w = threadIdx.x; w < NWD; w += kRleLbThreads) s_bits[w] = 0;
+        __syncthreads();
+        {
+            // this thread's run starts in the window, one OR per bitmap word
+            uint64_t s = st0;
+            unsigned cw = ~0u, acc = 0;
+#pragma unroll
+            for (unsigned k = 0; k < kRleLbRpt; k++) {
+                const uint64_t o = s - w0;  // start within the window (wraps when before it)
+                if (len[k] && o < kRleLbWin) {
+                    const unsigned wi = unsigned(o >> 5);
+                    if (wi != cw) {
+                        if (acc) atomicOr(&s_bits[cw], acc);
+                        cw = wi;
+                        acc = 0;
+                    }
+                    acc |= 1u << (o & 31u);
+                }
+                s += len[k];
+            }
+            if (acc) atomicOr(&s_bits[cw], acc);
+        }
+        __syncthreads();
+        const unsigned wr = unsigned(minu(kRleLbWin, rows - w0));
+        const unsigned nwd = (wr + 31) / 32, per = (nwd + NW - 1) / NW;
+        const unsigned u0 = wid * per, u1 = min(nwd, u0 + per);
+        if (u0 < u1) {
+            unsigned lo = 0, hi = kept;  // runs starting before the warp's first row
+            const uint64_t r0 = w0 + 32ull * u0;
+            while (lo < hi) {
+                const unsigned mid = (lo + hi) >> 1;
+                if (s_p[rle_lb_slot(mid)].y < r0) lo = mid + 1;
+                else hi = mid;
+            }
+            unsigned before = lo - 1u;  // index of the run holding the row before (wraps for none)
+            uint64_t *const o = out + base + w0 + lane;
+            for (unsigned u = u0; u < u1; u++) {
+                const unsigned bits = s_bits[u];
+                if (32 * u + lane < wr) o[32 * u] = s_p[rle_lb_slot(min(before + __popc(bits & incl), kept - 1))].x;
+                before += __popc(bits);
+            }
+        }
+        __syncthreads();
+    }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -762,6 +926,21 @@ static int decode_rle(const ms_col *in, uint64_t *d_out, ms_arena *a, cudaStream
     const uint64_t runs = in->size_used_byte / 16, n = in->count_values;
     if (!n) return MS_OK;
     if (!runs) return ms_fail(MS_ERR_CORRUPT, "rle column with values but no runs");
+    if (n <= kRleLbMaxMean * runs && (reinterpret_cast<uintptr_t>(in->data) & 15u) == 0) {
+        // short runs: one pass with a look-back
+        const uint64_t tiles = (runs + kRleLbTile - 1) / kRleLbTile;
+        RleTileState *state = arena_take_t<RleTileState>(a, tiles + 1);
+        unsigned *ticket = arena_take_t<unsigned>(a, 2);
+        if (!state || !ticket) return ms_fail(MS_ERR_NOMEM, "arena exhausted (rle decode)");
+        MS_CUDA_TRY(cudaMemsetAsync(state, 0, sizeof(RleTileState) * tiles, st));
+        MS_CUDA_TRY(cudaMemsetAsync(ticket, 0, sizeof(unsigned), st));
+        constexpr size_t smem = size_t(rle_lb_slot(kRleLbTile)) * 16;
+        MS_CUDA_TRY(cudaFuncSetAttribute(k_rle_expand_lb, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        k_rle_expand_lb<<<unsigned(tiles), kRleLbThreads, smem, st>>>((const uint64_t *)in->data, runs, n, state,
+                                                                      ticket, d_out, a->d_err);
+        MS_CUDA_TRY(cudaGetLastError());
+        return MS_OK;
+    }
     const unsigned tr = rle_tile_runs(n, runs);
     const uint64_t tiles = (runs + tr - 1) / tr;
     uint64_t *trows = arena_take_t<uint64_t>(a, tiles + 1);

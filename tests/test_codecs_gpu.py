@@ -202,14 +202,17 @@ def test_rle_decode_zero_length_runs(ms, arena, orc, mean_log2):
     assert np.array_equal(ms.morph(col, ms.uncompr_f).to_numpy(), want)
 
 
-def test_rle_decode_reports_inconsistent_lengths(ms, arena, orc):
-    """Run lengths that do not add up to the column's count are a corrupt
-    column: the decoder writes only rows inside the runs (nothing out of
-    bounds) and the call reports MS_ERR_CORRUPT."""
-    v = orc.runs(3, 5, 20, 50_000)
+@pytest.mark.parametrize("mean_log2", [0, 5])
+@pytest.mark.parametrize("delta", [-1, 1, 1 << 40])
+def test_rle_decode_reports_inconsistent_lengths(ms, arena, orc, mean_log2, delta):
+    """Run lengths that do not add up to the column's count (one run short,
+    one row long, 2^40 rows long) are a corrupt column: the decoder writes no
+    row past the column's end and the call reports MS_ERR_CORRUPT.  Runs of
+    one row take the one-pass decoder, runs of mean 32 the two-pass one."""
+    v = orc.runs(3, mean_log2, 20, 50_000) if mean_log2 else orc.uniform_bits(3, 20, 50_000)
     b, m = orc.compress(O.RLE, 0, v)
     pairs = b.view(np.uint64).copy()
-    pairs[1] -= 1  # the first run one row short
+    pairs[2 * 7 + 1] = np.uint64(int(pairs[2 * 7 + 1]) + delta)  # one run short or long
     col = ms.Column.from_bytes(ms.rle_f, pairs.view(np.uint8), m, arena)
     with pytest.raises(ms.MorphStoreError) as e:
         ms.morph(col, ms.uncompr_f)
