@@ -242,16 +242,27 @@ constexpr unsigned kRleEncTile = kRleEncThreads * kRleRowsPerThread;  // rows pe
 constexpr uint64_t kRleNone = ~uint64_t(0);
 enum : unsigned { kRleFlagAgg = 1, kRleFlagInc = 2 };
 
+// A tile's published values in two 64-bit words, each carrying the flag in
+// its low two bits (0: nothing yet, kRleFlagAgg: the tile's own values,
+// kRleFlagInc: the values over tiles [0, this tile]): r = runs << 2 | flag,
+// l = (last head + 1, 0 for none) << 2 | flag.  Each word is written and
+// read whole, so a value is never seen without its flag and no fence is
+// needed; a reader that sees the two words with different flags (one
+// already updated) reads again.
 struct RleTileState {
-    unsigned flag;
-    unsigned pad;
-    uint64_t agg_runs, agg_last;  // this tile's runs and last head (kRleNone: none)
-    uint64_t inc_runs, inc_last;  // the same over tiles [0, this tile]
+    unsigned long long r, l;
 };
 
+__device__ __forceinline__ void rle_publish(RleTileState *s, unsigned flag, uint64_t runs, uint64_t last) {
+    const unsigned long long r = (runs << 2) | flag;
+    const unsigned long long l = ((last == kRleNone ? 0 : last + 1) << 2) | flag;
+    asm volatile("st.relaxed.gpu.global.v2.u64 [%0], {%1, %2};" ::"l"(s), "l"(r), "l"(l) : "memory");
+}
+
 // Warp-wide look-back (warp 0 of the tile): lane i inspects tile j - i, 32
-// predecessors per step; the nearest one with an inclusive prefix ends the
-// walk.  Returns false if a predecessor never published (bounded spin).
+// predecessors per step, with one 16-byte load per lane and step; the
+// nearest one with an inclusive prefix ends the walk.  Returns false if a
+// predecessor never published (bounded spin).
 __device__ bool rle_lookback(const RleTileState *state, uint64_t tile, uint64_t &excl_runs, uint64_t &excl_last) {
     const unsigned lane = threadIdx.x & 31u;
     excl_runs = 0;
@@ -262,11 +273,14 @@ __device__ bool rle_lookback(const RleTileState *state, uint64_t tile, uint64_t 
         uint64_t cr = 0, cl = kRleNone;
         if (me >= 0) {
             const RleTileState *o = state + me;
-            unsigned spins = 0;
-            while ((f = *(volatile const unsigned *)&o->flag) == 0 && spins < kSpinLimit) spins++;
-            __threadfence();
-            cr = f == kRleFlagInc ? *(volatile const uint64_t *)&o->inc_runs : *(volatile const uint64_t *)&o->agg_runs;
-            cl = f == kRleFlagInc ? *(volatile const uint64_t *)&o->inc_last : *(volatile const uint64_t *)&o->agg_last;
+            unsigned long long r = 0, l = 0;
+            for (unsigned spins = 0; spins < kSpinLimit; spins++) {
+                asm volatile("ld.relaxed.gpu.global.v2.u64 {%0, %1}, [%2];" : "=l"(r), "=l"(l) : "l"(o) : "memory");
+                if ((r & 3u) != 0 && (r & 3u) == (l & 3u)) break;
+            }
+            f = (r & 3u) == (l & 3u) ? unsigned(r & 3u) : 0u;
+            cr = r >> 2;
+            cl = (l >> 2) ? (l >> 2) - 1 : kRleNone;
         }
         if (__any_sync(0xFFFFFFFFu, f == 0)) return false;
         const unsigned inc = __ballot_sync(0xFFFFFFFFu, f == kRleFlagInc);
@@ -344,27 +358,13 @@ __global__ void __launch_bounds__(kRleEncThreads) k_rle_encode(const uint64_t *_
         const uint64_t own_last = agg_last ? agg_last - 1 : kRleNone;
         uint64_t excl_runs = 0, excl_last = kRleNone;
         if (tile == 0) {
-            if (lane == 0) {
-                me->inc_runs = agg_runs;
-                me->inc_last = own_last;
-                __threadfence();
-                atomicExch(&me->flag, kRleFlagInc);
-            }
+            if (lane == 0) rle_publish(me, kRleFlagInc, agg_runs, own_last);
         } else {
-            if (lane == 0) {
-                me->agg_runs = agg_runs;
-                me->agg_last = own_last;
-                __threadfence();
-                atomicExch(&me->flag, kRleFlagAgg);
-            }
+            if (lane == 0) rle_publish(me, kRleFlagAgg, agg_runs, own_last);
             __syncwarp();
             if (!rle_lookback(state, tile, excl_runs, excl_last) && lane == 0) atomicOr(err, kErrTimeout);
-            if (lane == 0) {
-                me->inc_runs = excl_runs + agg_runs;
-                me->inc_last = own_last != kRleNone ? own_last : excl_last;
-                __threadfence();
-                atomicExch(&me->flag, kRleFlagInc);
-            }
+            if (lane == 0)
+                rle_publish(me, kRleFlagInc, excl_runs + agg_runs, own_last != kRleNone ? own_last : excl_last);
         }
         if (lane == 0) {
             s_excl_runs = excl_runs;
@@ -477,20 +477,12 @@ __global__ void __launch_bounds__(kRleStThreads) k_rle_encode_staged(const uint6
         const uint64_t own_last = agg_last ? agg_last - 1 : kRleNone;
         uint64_t excl_runs = 0, excl_last = kRleNone;
         if (tile > 0) {
-            if (lane == 0) {
-                me->agg_runs = agg_runs;
-                me->agg_last = own_last;
-                __threadfence();
-                atomicExch(&me->flag, kRleFlagAgg);
-            }
+            if (lane == 0) rle_publish(me, kRleFlagAgg, agg_runs, own_last);
             __syncwarp();
             if (!rle_lookback(state, tile, excl_runs, excl_last) && lane == 0) atomicOr(err, kErrTimeout);
         }
         if (lane == 0) {
-            me->inc_runs = excl_runs + agg_runs;
-            me->inc_last = own_last != kRleNone ? own_last : excl_last;
-            __threadfence();
-            atomicExch(&me->flag, kRleFlagInc);
+            rle_publish(me, kRleFlagInc, excl_runs + agg_runs, own_last != kRleNone ? own_last : excl_last);
             s_excl_runs = excl_runs;
             s_excl_last = excl_last;
             if (tile == ntiles - 1) {
@@ -810,20 +802,12 @@ __global__ void __launch_bounds__(kRleLbThreads, 2) k_rle_expand_lb(const uint64
     }
     // publish the tile's rows, then the rows before it
     RleTileState *me = state + tile;
-    if (threadIdx.x == 0 && tile > 0) {
-        me->agg_runs = agg;
-        me->agg_last = kRleNone;
-        __threadfence();
-        atomicExch(&me->flag, kRleFlagAgg);
-    }
+    if (threadIdx.x == 0 && tile > 0) rle_publish(me, kRleFlagAgg, agg, kRleNone);
     if (wid == 0) {
         uint64_t excl = 0, unused = kRleNone;
         if (tile > 0 && !rle_lookback(state, tile, excl, unused) && lane == 0) atomicOr(err, kErrTimeout);
         if (lane == 0) {
-            me->inc_runs = excl + agg;
-            me->inc_last = kRleNone;
-            __threadfence();
-            atomicExch(&me->flag, kRleFlagInc);
+            rle_publish(me, kRleFlagInc, excl + agg, kRleNone);
             s_base = excl;
             if (tile == ntiles - 1 && excl + agg != n) atomicOr(err, kErrCorrupt);
         }
