@@ -210,7 +210,7 @@ __global__ void k_finish_sizes(uint64_t nb, Layout L, const uint32_t *__restrict
 }
 
 // --- decompression ------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_decode_all(ColView c, uint64_t *__restrict__ out, unsigned *err) {
+__global__ void __launch_bounds__(256, 3) k_decode_all(ColView c, uint64_t *__restrict__ out, unsigned *err) {
     const unsigned lane = threadIdx.x & 31u, l = lane & 7u, q = lane >> 3;
     const uint64_t nbt = c.nblocks_total();
     for (uint64_t b = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) / 32; b < nbt;

@@ -37,10 +37,18 @@ struct ColView {
 // values with a lane-wise running sum -- thread-local over its 16 slots,
 // across the four quarters of the lane by shuffles, plus the block's
 // carry-in (delta.h:285-347).
+// `side` is the block's reference (for_f) or this lane's carry-in (delta_f),
+// loaded by cascade_side before the unpack so that its latency overlaps it.
+__device__ __forceinline__ uint64_t cascade_side(const ColView &c, uint64_t b, unsigned l) {
+    if (c.fmt == MS_FMT_FOR_DVBP) return __ldg(c.aux + (b >> 1));
+    if (c.fmt == MS_FMT_DELTA_DVBP) return __ldg(c.carry + b * 8 + l);
+    return 0;
+}
+
 __device__ __forceinline__ void apply_cascade(const ColView &c, uint64_t b, unsigned l, unsigned q,
-                                              uint64_t (&v)[16]) {
+                                              uint64_t (&v)[16], uint64_t side) {
     if (c.fmt == MS_FMT_FOR_DVBP) {
-        const uint64_t ref = __ldg(c.aux + (b >> 1));
+        const uint64_t ref = side;
 #pragma unroll
         for (int k = 0; k < 16; k++) v[k] += ref;
     } else if (c.fmt == MS_FMT_DELTA_DVBP) {
@@ -51,7 +59,7 @@ __device__ __forceinline__ void apply_cascade(const ColView &c, uint64_t b, unsi
         uint64_t pre = q >= 1 ? up : 0;
         const uint64_t up2 = __shfl_up_sync(0xFFFFFFFFu, tot + pre, 16);
         pre += q >= 2 ? up2 : 0;
-        pre += __ldg(c.carry + b * 8 + l);
+        pre += side;
 #pragma unroll
         for (int k = 0; k < 16; k++) v[k] += pre;
     }
@@ -75,8 +83,9 @@ __device__ __forceinline__ bool decode_block(const ColView &c, uint64_t b, unsig
             off = idx_off(e);
             bw = idx_bw(e);
         }
+        const uint64_t side = cascade_side(c, b, l);
         const bool ok = vbp_decode16_rt(bw, reinterpret_cast<const uint64_t *>(c.data + off), l, q, v);
-        apply_cascade(c, b, l, q, v);
+        apply_cascade(c, b, l, q, v, side);
         return ok;
     }
     // uncompressed rows

@@ -311,7 +311,7 @@ __global__ void k_walk_for(const uint8_t *__restrict__ d, uint64_t compr, uint64
 }
 
 // delta carries: per 512-block, lane-wise sums of the decoded deltas.
-__global__ void __launch_bounds__(256) k_delta_block_sums(ms::ColView c, uint64_t *__restrict__ sums, unsigned *err) {
+__global__ void __launch_bounds__(256, 3) k_delta_block_sums(ms::ColView c, uint64_t *__restrict__ sums, unsigned *err) {
     const unsigned lane = threadIdx.x & 31u, l = lane & 7u, q = lane >> 3;
     const uint64_t nb = c.nb();
     ms::ColView raw = c;

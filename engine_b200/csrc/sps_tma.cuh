@@ -230,19 +230,21 @@ __global__ void __launch_bounds__(32 * (W + 1), 1)
             for (unsigned j = j0; j < T; j += W) {
                 const uint64_t blk = b0 + j;
                 uint64_t v[16];
+                const uint64_t xside = cascade_side(x, blk, l);
                 ok &= vbp_decode16_rt<true>(xbw[st * kMaxTile + j],
                                             reinterpret_cast<const uint64_t *>(ring + xoff[st * kMaxTile + j]), l,
                                             q, v);
-                apply_cascade(x, blk, l, q, v);
+                apply_cascade(x, blk, l, q, v, xside);
                 const unsigned m = select_mask(x, blk, l, q, v, 0xFFFFu, cmp, val);
                 s_cnt += __popc(m);
                 if (kHasY) {
                     if (__any_sync(0xFFFFFFFFu, m != 0)) {
                         uint64_t w[16];
+                        const uint64_t yside = cascade_side(y, blk, l);
                         ok &= vbp_decode16_rt<true>(ybw[st * kMaxTile + j],
                                                     reinterpret_cast<const uint64_t *>(ring + yoff[st * kMaxTile + j]),
                                                     l, q, w);
-                        apply_cascade(y, blk, l, q, w);
+                        apply_cascade(y, blk, l, q, w, yside);
 #pragma unroll
                         for (int k = 0; k < 16; k++) s_sum += ((m >> k) & 1u) ? w[k] : 0;
                     }
