@@ -267,6 +267,18 @@ __global__ void __launch_bounds__(32 * (W + 1), 1)
         unsigned t = 0;
         for (;; t++) {
             const unsigned st = t % S, use = t / S;
+            // the next tile's block locations are requested before waiting
+            // for its stage, so the index loads overlap the wait
+            const uint64_t blk = b + lane;
+            const bool valid = blk < b_hi;
+            uint64_t off[kQCols], len[kQCols], x0[kQCols];
+            unsigned bw[kQCols];
+#pragma unroll
+            for (unsigned c = 0; c < kQCols; c++) {
+                off[c] = 0;
+                bw[c] = 0;
+                if (valid) blk_loc(*cols[c], blk, off[c], bw[c]);
+            }
             if (use > 0 && !mbar_wait(empty + st, (use - 1) & 1u)) {
                 ok = false;
                 break;
@@ -279,16 +291,9 @@ __global__ void __launch_bounds__(32 * (W + 1), 1)
                 t++;
                 break;
             }
-            const uint64_t blk = b + lane;
-            const bool valid = blk < b_hi;
-            uint64_t off[kQCols], len[kQCols], x0[kQCols];
-            unsigned bw[kQCols];
             uint64_t need = 0;
 #pragma unroll
             for (unsigned c = 0; c < kQCols; c++) {
-                off[c] = 0;
-                bw[c] = 0;
-                if (valid) blk_loc(*cols[c], blk, off[c], bw[c]);
                 x0[c] = __shfl_sync(0xFFFFFFFFu, off[c], 0);
                 len[c] = valid ? off[c] + 64ull * bw[c] - x0[c] : 0;
                 need += align_up(len[c], 128);

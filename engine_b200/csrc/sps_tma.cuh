@@ -92,6 +92,16 @@ __global__ void __launch_bounds__(32 * (W + 1), 1)
         unsigned t = 0;  // tiles issued
         for (;; t++) {
             const unsigned st = t % S, use = t / S;
+            // the next tile's block locations are requested before waiting
+            // for its stage, so the index loads overlap the wait
+            const uint64_t blk = b + lane;
+            const bool valid = blk < b_hi && lane < cfg.max_tile;
+            uint64_t xo = 0, yo = 0;
+            unsigned xw = 0, yw = 0;
+            if (valid) {
+                blk_loc(xs, blk, xo, xw);
+                if (kHasY) blk_loc(ys, blk, yo, yw);
+            }
             if (use > 0 && !mbar_wait(empty + st, (use - 1) & 1u)) {
                 ok = false;
                 break;
@@ -103,14 +113,6 @@ __global__ void __launch_bounds__(32 * (W + 1), 1)
                 }
                 t++;
                 break;
-            }
-            const uint64_t blk = b + lane;
-            const bool valid = blk < b_hi && lane < cfg.max_tile;
-            uint64_t xo = 0, yo = 0;
-            unsigned xw = 0, yw = 0;
-            if (valid) {
-                blk_loc(xs, blk, xo, xw);
-                if (kHasY) blk_loc(ys, blk, yo, yw);
             }
             const uint64_t x0 = __shfl_sync(0xFFFFFFFFu, xo, 0), y0 = __shfl_sync(0xFFFFFFFFu, yo, 0);
             const uint64_t xlen = valid ? xo + 64ull * xw - x0 : 0;
