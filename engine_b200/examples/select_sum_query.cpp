@@ -1,6 +1,13 @@
-// select_sum_query.cpp -- the reference's example query
-// (src/examples/select_sum_query.cpp:51-108) written against the drop-in
-// header: only the include and the processing style differ.
+// select_sum_query.cpp -- the query of the reference's example
+// (src/examples/select_sum_query.cpp:51-108) written for the device-resident
+// C++ layer (morphstore_b200/morphstore.h), which keeps columns on the GPU
+// between operators.  It differs from the reference's file: the base data
+// come from a seeded splitmix64 generator instead of generate_with_distr,
+// both columns are morphed to dynamic_vbp on the device first, and the
+// program checks its sum instead of printing it.  The reference's own file,
+// with only its processing style changed to gpu_b200, is built from the
+// reference's sources through morphstore_b200/ve_gpu_b200.h by
+// engine_b200/build.py.
 //   SELECT SUM(baseCol2) WHERE baseCol1 = 150
 // Base data: baseCol1 uniform in [100, 199], baseCol2 uniform in [0, 10]
 // (seeded, counter-based splitmix64), compressed as dynamic_vbp on the device.
