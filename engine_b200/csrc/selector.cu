@@ -391,6 +391,7 @@ __global__ void __launch_bounds__(256) k_sel_features(const uint64_t *__restrict
         }
         float f[kSelNF];
         const float nv = 256.f, ndf = float(__reduce_add_sync(0xFFFFFFFFu, nd));
+        const float rnd = 1.f / ndf;  // one division; the delta features multiply by it
         // two counters per 32-bit word (16-bit fields: warp sums stay below 2^16)
 #pragma unroll
         for (int k = 0; k < 4; k++) {
@@ -399,22 +400,27 @@ __global__ void __launch_bounds__(256) k_sel_features(const uint64_t *__restrict
             const unsigned sv = __reduce_add_sync(0xFFFFFFFFu, pv), sd = __reduce_add_sync(0xFFFFFFFFu, pd);
             f[2 * k] = float(sv & 0xFFFFu) / nv;
             f[2 * k + 1] = float(sv >> 16) / nv;
-            f[8 + 2 * k] = float(sd & 0xFFFFu) / ndf;
-            f[8 + 2 * k + 1] = float(sd >> 16) / ndf;
+            f[8 + 2 * k] = float(sd & 0xFFFFu) * rnd;
+            f[8 + 2 * k + 1] = float(sd >> 16) * rnd;
         }
         f[16] = float(__reduce_max_sync(0xFFFFFFFFu, vmax)) / 64.f;
         f[17] = float(__reduce_min_sync(0xFFFFFFFFu, vmin)) / 64.f;
-#pragma unroll
-        for (int s = 16; s > 0; s >>= 1) {
-            umax = maxu(umax, __shfl_xor_sync(0xFFFFFFFFu, umax, s));
-            umin = minu(umin, __shfl_xor_sync(0xFFFFFFFFu, umin, s));
+        {
+            // 64-bit warp max / min from 32-bit reductions: high words first,
+            // then the low words of the lanes that hold the extreme high word
+            const unsigned xh = __reduce_max_sync(0xFFFFFFFFu, unsigned(umax >> 32));
+            const unsigned xl = __reduce_max_sync(0xFFFFFFFFu, unsigned(umax >> 32) == xh ? unsigned(umax) : 0u);
+            const unsigned nh = __reduce_min_sync(0xFFFFFFFFu, unsigned(umin >> 32));
+            const unsigned nl = __reduce_min_sync(0xFFFFFFFFu, unsigned(umin >> 32) == nh ? unsigned(umin) : ~0u);
+            umax = uint64_t(xh) << 32 | xl;
+            umin = uint64_t(nh) << 32 | nl;
         }
         f[18] = float(effective_bitwidth(umax - umin)) / 64.f;
         f[19] = float(__reduce_max_sync(0xFFFFFFFFu, dmax)) / 64.f;
-        f[20] = float(__reduce_add_sync(0xFFFFFFFFu, neg)) / ndf;
+        f[20] = float(__reduce_add_sync(0xFFFFFFFFu, neg)) * rnd;
         const float hr = float(__reduce_add_sync(0xFFFFFFFFu, heads)) / 252.f;
         f[21] = hr;
-        f[22] = float(__reduce_add_sync(0xFFFFFFFFu, zd)) / ndf;
+        f[22] = float(__reduce_add_sync(0xFFFFFFFFu, zd)) * rnd;
         f[23] = float(__reduce_add_sync(0xFFFFFFFFu, vsum)) / (nv * 64.f);
 #pragma unroll
         for (int c = 0; c < 4; c++) {
